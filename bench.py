@@ -1,0 +1,349 @@
+"""Benchmark: audio-hours/s of STFT -> mel -> MFCC on B200.
+
+Workload (default): 256 clips x 30 s at 22050 Hz (661500 samples each) of
+seeded synthetic music-like audio; n_fft 2048, hop 512, Hann, centred with
+zero padding, 128 Slaney mels (0-11025 Hz), power_to_db(ref 1, amin 1e-10,
+top_db 80), 20 MFCC (DCT-II ortho).  One step = the whole batch through the
+batched plan.  Inputs (677 MB per GPU) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+  value    device-resident throughput (inputs already in HBM), CUDA events
+           around the K timed steps on the launching stream, max over ranks;
+  e2e      the same metric through the public plan API with pinned host
+           buffers: H2D of every clip + kernels + D2H of every MFCC per step;
+  roofline dominant kernel (the frame kernel) against measured HBM bandwidth:
+           algorithmic bytes = 4*L (audio read) + 4*n_mels*T (log-mel write)
+           per clip, divided by its in-region CUDA-event duration;
+  cpu_baseline  the float32 C port of the reference's CPU path on a bounded
+           sample of the same clips, all host cores.
+
+`--impl reference` times that CPU port alone (the reference's own Swift +
+Accelerate path cannot be built on Linux) on bounded samples of the same
+workload and prints the same JSON line with "impl": "reference".
+Multi-GPU (torchrun): every rank processes its own 256 clips (weak scaling);
+no collective touches the data path.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "audio-hours/sec STFT->mel->MFCC at <=1e-3 dB vs FP64"
+UNIT = "audio-hours/s"
+SR, N_FFT, HOP, N_MELS, N_MFCC = 22050, 2048, 512, 128, 20
+CLIP_SAMPLES = 661500
+N_CLIPS = 256
+
+
+def workload_config(n_clips):
+    return {
+        "workload": f"{n_clips} clips x 30 s @22050 Hz, n_fft 2048, hop 512, 128 mels, 20 MFCC",
+        "n_clips": n_clips, "clip_samples": CLIP_SAMPLES, "sample_rate": SR, "n_fft": N_FFT,
+        "hop_length": HOP, "n_mels": N_MELS, "n_mfcc": N_MFCC, "center": True,
+        "pad_mode": "constant", "top_db": 80.0,
+        "l2": "inputs 677 MB per GPU > 126 MB L2 (no flush needed)",
+    }
+
+
+def make_clips(n, seed0):
+    from metalmom_b200 import synth
+    return [synth.music_clip(CLIP_SAMPLES, SR, seed0 + i) for i in range(n)]
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason samples while a region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def cpu_baseline(clips, n_sample):
+    from oracle import refcpu
+    sample = clips[:n_sample]
+    threads = os.cpu_count() or 1
+    refcpu.mfcc_batch(sample[:min(len(sample), threads)], sr=SR, n_fft=N_FFT, hop=HOP,
+                      n_mels=N_MELS, n_mfcc=N_MFCC, n_threads=threads)  # warm caches
+    t0 = time.perf_counter()
+    refcpu.mfcc_batch(sample, sr=SR, n_fft=N_FFT, hop=HOP, n_mels=N_MELS, n_mfcc=N_MFCC,
+                      n_threads=threads)
+    dt = time.perf_counter() - t0
+    hours = len(sample) * CLIP_SAMPLES / SR / 3600.0
+    return {"value": hours / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(sample)} of the {len(clips)} clips (30 s each), one clip per thread; "
+                      "float32 C port of the reference CPU algorithm (radix-2 FFT, dense mel GEMM)",
+            "seconds": dt}
+
+
+class _DevView:
+    """A float32 device range as a torch tensor (no copy) via __cuda_array_interface__."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False),
+                                         "version": 2}
+
+
+def _device_floats(ptr, n):
+    import torch
+    return torch.as_tensor(_DevView(ptr, n), device="cuda").cpu().numpy().copy()
+
+
+def baseline_leg(plan, clips, world, args):
+    """The checker and the CPU baseline (rank 0): FP64 check of this run's own
+    mel-dB / MFCC output on two clips, then the CPU port timed at N=1."""
+    from oracle import oracle as O
+    out = {}
+    mel_err, mfcc_err = 0.0, 0.0
+    idx = [0, len(clips) - 1]
+    frame0 = np.concatenate([[0], np.cumsum(plan.frames)])
+    for i in idx:
+        T = plan.frames[i]
+        mel = _device_floats(plan.device_mel_db + 4 * int(frame0[i]) * N_MELS, T * N_MELS)
+        mel = mel.reshape(T, N_MELS).T.astype(np.float64)
+        mel = np.maximum(mel, plan.clip_max_db(i) - 80.0)
+        exp_db = O.mel_db(clips[i], SR, N_FFT, HOP, N_FFT, True, N_MELS)
+        mel_err = max(mel_err, float(np.abs(mel - exp_db).max()))
+        got = _device_floats(plan.device_output + 4 * plan.out_offsets[i], N_MFCC * T)
+        exp = O.mfcc(clips[i], SR, N_MFCC, N_FFT, HOP, N_FFT, N_MELS)
+        mfcc_err = max(mfcc_err, O.mfcc_rel_error(got.reshape(N_MFCC, T), exp))
+    out["accuracy"] = {"mel_db_max_abs_err_db": mel_err, "mfcc_max_err_rel_to_max": mfcc_err,
+                       "clips_checked": len(idx), "oracle": "float64 NumPy restatement"}
+    if world == 1:
+        out["cpu_baseline"] = cpu_baseline(clips, args.cpu_clips)
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import metalmom_b200 as M
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    n_clips = args.clips
+    clips = make_clips(n_clips, seed0=1000 * rank)
+    lengths = [len(c) for c in clips]
+    plan = M.Plan(lengths, sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    # pinned host buffers for the end-to-end leg
+    pin_in = [torch.from_numpy(c).pin_memory() for c in clips]
+    in_np = [t.numpy() for t in pin_in]
+    pin_out = [torch.empty((plan.rows, f), dtype=torch.float32).pin_memory() for f in plan.frames]
+    out_np = [t.numpy() for t in pin_out]
+    plan.execute_host(in_np, out_np, stream=sh)  # uploads the inputs once
+    torch.cuda.synchronize()
+
+    hours_per_step = n_clips * CLIP_SAMPLES / SR / 3600.0
+    K, W = args.steps, args.warmup
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident timed region
+    for i in range(W):
+        plan.execute_timed(i % 64, stream=sh)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        start.record(stream)
+        for i in range(K):
+            plan.execute_timed(i % 64, stream=sh)
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    stage = np.array([plan.stage_ms(i) for i in range(min(K, 64))])
+    frame_ms = float(stage[:, 1].mean())
+    dct_ms = float(stage[:, 2].mean())
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / K
+    value = hours_per_step * world / (ms_step / 1e3)
+
+    # ---- end-to-end through the public API (pinned host in/out every step)
+    for _ in range(max(1, W // 2)):
+        plan.execute_host(in_np, out_np, stream=sh)
+    torch.cuda.synchronize()
+    barrier()
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ke = max(1, min(K, args.e2e_steps))
+    e_start.record(stream)
+    for _ in range(ke):
+        plan.execute_host(in_np, out_np, stream=sh)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e_start.elapsed_time(e_end)
+    if dist is not None:
+        t = torch.tensor([e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    e2e_value = hours_per_step * world / (e_ms / ke / 1e3)
+    h2d = sum(c.nbytes for c in in_np)
+    d2h = sum(o.nbytes for o in out_np)
+
+    result = None
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except Exception:
+            pass
+        hbm = peaks.get("hbm_gbs")
+        peak_note = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        T_total = plan.total_frames
+        alg_bytes = 4.0 * sum(lengths) + 4.0 * N_MELS * T_total
+        achieved = alg_bytes / (frame_ms / 1e3) / 1e9
+        pipe_bytes = 4.0 * sum(lengths) + 4.0 * N_MFCC * T_total
+        flops_fft = 2.5 * N_FFT * np.log2(N_FFT) * T_total
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "frame_kernel_traffic.json")
+        if os.path.exists(tp):
+            try:
+                traffic = json.load(open(tp)).get("bytes_per_launch")
+            except Exception:
+                traffic = None
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": W, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded music-like clips)",
+            "config": dict(workload_config(n_clips), parallelism=f"clip-sharded x{world}" if world > 1 else "1 GPU"),
+            "roofline": {"bound": "hbm", "kernel": "frontend_kernel<11,4,MELDB>",
+                         "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": peak_note, "traffic": traffic,
+                         "kernel_ms": frame_ms, "dct_ms": dct_ms,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "pipeline_frac": pipe_bytes / (ms_step / 1e3) / 1e9 / hbm,
+                         "fp32_fft_tflops": flops_fft / (frame_ms / 1e3) / 1e12},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": ke,
+                    "api": "Plan.execute_host (mm_plan_execute_host)"},
+            "clocks": clk.summary(),
+            "gpu_launches": K * plan.kernel_launches,
+        }
+        if not args.no_cpu:
+            result.update(baseline_leg(plan, clips, world, args))
+    plan.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return result
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    from oracle import refcpu
+    threads = os.cpu_count() or 1
+    n = args.ref_clips
+    clips = make_clips(n, seed0=0)
+    kw = dict(sr=SR, n_fft=N_FFT, hop=HOP, n_mels=N_MELS, n_mfcc=N_MFCC, n_threads=threads)
+    for _ in range(args.warmup):
+        refcpu.mfcc_batch(clips, **kw)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        refcpu.mfcc_batch(clips, **kw)
+        times.append(time.perf_counter() - t0)
+    dt = float(np.mean(times))
+    hours = n * CLIP_SAMPLES / SR / 3600.0
+    v = hours / dt
+    sample = (f"{n} of the {N_CLIPS} workload clips per step (30 s each), one clip per thread")
+    return {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(N_CLIPS), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "MetalMom's CPU path is Swift + Apple Accelerate and cannot be built on Linux; "
+                "this arm times its float32 C port (oracle/refcpu.c) on the host cores.",
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--clips", type=int, default=N_CLIPS)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-clips", type=int, default=128)
+    ap.add_argument("--ref-clips", type=int, default=32)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        res = run_reference(args, rank)
+    else:
+        res = run_ours(args, rank, world, local_rank)
+    if rank == 0 and res is not None:
+        print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()

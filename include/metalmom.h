@@ -1,0 +1,171 @@
+/*
+ * metalmom.h -- C ABI of the B200 spectral front end (libmetalmom.so).
+ *
+ * The first part is a byte-compatible restatement of the MetalMom bridge
+ * header (Sources/MetalMomCBridge/include/metalmom.h in the MetalMom project)
+ * for the entry points of the STFT -> mel -> MFCC path.  Callers written
+ * against MetalMom (its Python cffi layer, Swift hosts) bind these symbols
+ * unchanged.  The second part adds batched, device-resident and serving entry
+ * points that have no counterpart in MetalMom.
+ *
+ * Every compute entry point runs on the CUDA device that is current for the
+ * calling thread; there is no CPU fallback.  Without a usable GPU the compute
+ * calls return MM_ERR_METAL_UNAVAILABLE (the reference's "no Metal device"
+ * code, reused as "no CUDA device").
+ */
+#ifndef METALMOM_H
+#define METALMOM_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__) && defined(MM_BUILDING_LIBRARY)
+#define MM_API __attribute__((visibility("default")))
+#else
+#define MM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (reference metalmom.h:6-11). */
+#define MM_OK 0
+#define MM_ERR_INVALID_INPUT -1
+#define MM_ERR_METAL_UNAVAILABLE -2
+#define MM_ERR_ALLOC_FAILED -3
+#define MM_ERR_INTERNAL -4
+
+/* Result buffer (reference metalmom.h:14-20): 88 bytes, data malloc'd by the
+ * library and released with mm_buffer_free. */
+typedef struct {
+    float* data;
+    int64_t shape[8];
+    int32_t ndim;
+    int32_t dtype; /* 0 = float32 */
+    int64_t count;
+} MMBuffer;
+
+/* STFT parameters (reference metalmom.h:23-28). */
+typedef struct {
+    int32_t n_fft;
+    int32_t hop_length;
+    int32_t win_length;
+    int32_t center; /* 1 = pad n_fft/2 zeros on both sides */
+} MMSTFTParams;
+
+/* Opaque context.  Not thread-safe: create one per thread (reference
+ * metalmom.h:30-31). */
+typedef void* mm_context;
+
+/* ---- Reference entry points ------------------------------------------- */
+
+/* Replaces MetalMomBridge/Bridge.swift:22 (mm_init). */
+MM_API mm_context mm_init(void);
+
+/* Replaces Bridge.swift:33 (mm_destroy); destroying twice is a no-op. */
+MM_API void mm_destroy(mm_context ctx);
+
+/* Replaces Bridge.swift:44 (mm_stft): magnitude |X|, shape [n_fft/2+1, n_frames].
+ * hop_length / win_length are used as given (no sentinels), as in the
+ * reference; n_fft must be a power of two.  hop_length <= 0 is rejected with
+ * MM_ERR_INVALID_INPUT (the reference divides by it). */
+MM_API int32_t mm_stft(mm_context ctx, const float* signal_data, int64_t signal_length,
+                int32_t sample_rate, const MMSTFTParams* params, MMBuffer* out);
+
+/* Replaces Bridge.swift:225 (mm_amplitude_to_db): 20*log10(max(x,amin)/ref),
+ * floored at max-top_db when top_db > 0.  Output ndim 1, shape [count]. */
+MM_API int32_t mm_amplitude_to_db(mm_context ctx, const float* data, int64_t count,
+                           float ref, float amin, float top_db, MMBuffer* out);
+
+/* Replaces Bridge.swift:267 (mm_power_to_db): 10*log10(max(x,amin)/ref),
+ * floored at max-top_db when top_db > 0.  Output ndim 1, shape [count]. */
+MM_API int32_t mm_power_to_db(mm_context ctx, const float* data, int64_t count,
+                       float ref, float amin, float top_db, MMBuffer* out);
+
+/* Replaces Bridge.swift:310 (mm_mel_spectrogram): FB @ |X|^power, shape
+ * [n_mels, n_frames].  Sentinels: hop<=0 -> n_fft/4, win<=0 -> n_fft,
+ * f_max<=0 -> sr/2. */
+MM_API int32_t mm_mel_spectrogram(mm_context ctx, const float* signal_data, int64_t signal_length,
+                           int32_t sample_rate, int32_t n_fft, int32_t hop_length,
+                           int32_t win_length, int32_t center, float power,
+                           int32_t n_mels, float f_min, float f_max, MMBuffer* out);
+
+/* Replaces Bridge.swift:402 (mm_mfcc): DCT-II ortho of power_to_db(mel, ref 1,
+ * amin 1e-10, top_db 80), shape [min(n_mfcc, n_mels), n_frames]. */
+MM_API int32_t mm_mfcc(mm_context ctx, const float* signal_data, int64_t signal_length,
+                int32_t sample_rate, int32_t n_mfcc, int32_t n_fft,
+                int32_t hop_length, int32_t win_length,
+                int32_t n_mels, float f_min, float f_max,
+                int32_t center, MMBuffer* out);
+
+/* Replaces Bridge.swift:3695 (mm_buffer_free): frees data, zeroes the struct;
+ * NULL-safe. */
+MM_API void mm_buffer_free(MMBuffer* buf);
+
+/* ---- Additive entry points (no counterpart in the reference) ----------- */
+
+#define MM_PAD_CONSTANT 0 /* zeros: the reference's centering */
+#define MM_PAD_REFLECT 1  /* mirror without repeating the edge sample */
+
+/* One front-end parameter group.  Sentinels as in mm_mfcc. */
+typedef struct {
+    int32_t sample_rate;
+    int32_t n_fft;
+    int32_t hop_length; /* <= 0: n_fft/4 */
+    int32_t win_length; /* <= 0: n_fft */
+    int32_t center;
+    int32_t pad_mode;   /* MM_PAD_CONSTANT or MM_PAD_REFLECT */
+    int32_t n_mels;
+    int32_t n_mfcc;
+    float f_min;
+    float f_max;        /* <= 0: sr/2 */
+    float top_db;       /* <= 0: no floor; mm_mfcc uses 80 */
+    int32_t reserved;
+} MMFrontEndParams;
+
+/* MFCC of n_clips clips of any lengths in one batched launch sequence.
+ * outs[i] receives [min(n_mfcc,n_mels), n_frames_i]; free each with
+ * mm_buffer_free. */
+MM_API int32_t mm_mfcc_batch(mm_context ctx, const float* const* signals, const int64_t* lengths,
+                      int32_t n_clips, const MMFrontEndParams* params, MMBuffer* outs);
+
+/* A plan fixes the parameters and clip lengths of a batch, keeps its tables
+ * and device buffers resident and captures its launches in a CUDA graph.
+ * Inputs live in one device buffer (clip i at mm_plan_input_offset(i)
+ * floats); outputs in another ([rows, n_frames_i] at mm_plan_output_offset).
+ * Streams are passed as void* (a cudaStream_t; NULL = the plan's own). */
+typedef void* mm_plan;
+
+MM_API mm_plan mm_plan_create(mm_context ctx, const MMFrontEndParams* params,
+                       const int64_t* lengths, int32_t n_clips, int32_t* status);
+MM_API void mm_plan_destroy(mm_plan plan);
+MM_API float* mm_plan_device_input(mm_plan plan);
+MM_API float* mm_plan_device_output(mm_plan plan);
+MM_API int64_t mm_plan_input_offset(mm_plan plan, int32_t clip);
+MM_API int64_t mm_plan_output_offset(mm_plan plan, int32_t clip);
+MM_API int64_t mm_plan_clip_frames(mm_plan plan, int32_t clip);
+MM_API int32_t mm_plan_rows(mm_plan plan);
+MM_API int64_t mm_plan_total_frames(mm_plan plan);
+MM_API int32_t mm_plan_kernel_launches(mm_plan plan);
+/* The log-mel intermediate of the last execution, frame-major
+ * [total_frames, n_mels] (clip i's frames start at the sum of the earlier
+ * clips' frame counts), before the top_db floor; and clip i's maximum dB. */
+MM_API float* mm_plan_device_mel_db(mm_plan plan);
+MM_API int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float* max_db);
+/* Replays the captured graph on `stream`. */
+MM_API int32_t mm_plan_execute(mm_plan plan, void* stream);
+/* Same kernels launched directly, with CUDA events recorded around each of
+ * the three stages into timing slot `slot` (0..63); read them after the
+ * stream has synchronised with mm_plan_stage_ms. */
+MM_API int32_t mm_plan_execute_timed(mm_plan plan, void* stream, int32_t slot);
+MM_API int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float* ms3);
+/* Host buffers in and out: copies signals[i] into the device input, runs the
+ * plan, copies every clip's result into outs[i] and synchronises. */
+MM_API int32_t mm_plan_execute_host(mm_plan plan, const float* const* signals, float* const* outs,
+                             void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* METALMOM_H */

@@ -1,0 +1,14 @@
+"""B200-native spectral front end with MetalMom's API.
+
+``stft``, ``melspectrogram``, ``mfcc``, ``power_to_db`` and ``amplitude_to_db``
+keep the names, defaults and error behaviour of MetalMom's Python package and
+run on the GPU through ``libmetalmom.so``; ``mfcc_batch`` and ``Plan`` add a
+batched, device-resident path.
+"""
+
+from .core import stft
+from .feature import amplitude_to_db, melspectrogram, mfcc, power_to_db
+from .batch import Plan, frontend_params, mfcc_batch
+
+__all__ = ["stft", "melspectrogram", "mfcc", "power_to_db", "amplitude_to_db",
+           "mfcc_batch", "Plan", "frontend_params"]

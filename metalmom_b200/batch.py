@@ -1,0 +1,144 @@
+"""Batched MFCC over many clips (additive API, no counterpart in MetalMom).
+
+``mfcc_batch`` is one call over clips of any lengths.  ``Plan`` keeps a fixed
+batch (parameters + clip lengths) resident on the device with its launches
+captured in a CUDA graph; inputs and outputs live in device buffers whose
+addresses and per-clip offsets the plan exposes.
+"""
+
+import numpy as np
+
+from ._buffer import buffer_to_numpy
+from ._native import ffi, lib
+
+
+def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, center=True,
+                    pad_mode="constant", n_mels=128, n_mfcc=20, fmin=0.0, fmax=None,
+                    top_db=80.0):
+    """An ``MMFrontEndParams`` struct (sentinels: None -> reference defaults)."""
+    p = ffi.new("MMFrontEndParams*")
+    p.sample_rate = sr
+    p.n_fft = n_fft
+    p.hop_length = hop_length if hop_length is not None else 0
+    p.win_length = win_length if win_length is not None else 0
+    p.center = 1 if center else 0
+    p.pad_mode = {"constant": lib.MM_PAD_CONSTANT, "reflect": lib.MM_PAD_REFLECT}[pad_mode]
+    p.n_mels = n_mels
+    p.n_mfcc = n_mfcc
+    p.f_min = fmin
+    p.f_max = float(fmax) if fmax is not None else 0.0
+    p.top_db = float(top_db) if top_db is not None else 0.0
+    return p
+
+
+def mfcc_batch(clips, **params):
+    """MFCC of every clip in one batched launch sequence; returns a list of arrays."""
+    clips = [np.ascontiguousarray(c, dtype=np.float32) for c in clips]
+    n = len(clips)
+    if n == 0:
+        return []
+    p = frontend_params(**params)
+    ptrs = ffi.new("const float*[]", [ffi.cast("const float*", c.ctypes.data) for c in clips])
+    lens = ffi.new("int64_t[]", [len(c) for c in clips])
+    outs = ffi.new("MMBuffer[]", n)
+    ctx = lib.mm_init()
+    try:
+        status = lib.mm_mfcc_batch(ctx, ptrs, lens, n, p, outs)
+        if status != 0:
+            raise RuntimeError(f"mm_mfcc_batch failed with status {status}")
+        return [buffer_to_numpy(outs[i]) for i in range(n)]
+    finally:
+        lib.mm_destroy(ctx)
+
+
+class Plan:
+    """A resident, graph-captured batch of fixed clip lengths."""
+
+    def __init__(self, lengths, **params):
+        self.lengths = [int(x) for x in lengths]
+        self._params = frontend_params(**params)
+        self._ctx = lib.mm_init()
+        st = ffi.new("int32_t*")
+        lens = ffi.new("int64_t[]", self.lengths)
+        self._plan = lib.mm_plan_create(self._ctx, self._params, lens, len(self.lengths), st)
+        if self._plan == ffi.NULL:
+            lib.mm_destroy(self._ctx)
+            raise RuntimeError(f"mm_plan_create failed with status {st[0]}")
+        self.n = len(self.lengths)
+        self.rows = lib.mm_plan_rows(self._plan)
+        self.frames = [lib.mm_plan_clip_frames(self._plan, i) for i in range(self.n)]
+        self.in_offsets = [lib.mm_plan_input_offset(self._plan, i) for i in range(self.n)]
+        self.out_offsets = [lib.mm_plan_output_offset(self._plan, i) for i in range(self.n)]
+        self.total_frames = lib.mm_plan_total_frames(self._plan)
+        self.kernel_launches = lib.mm_plan_kernel_launches(self._plan)
+
+    @property
+    def device_input(self) -> int:
+        return int(ffi.cast("uintptr_t", lib.mm_plan_device_input(self._plan)))
+
+    @property
+    def device_output(self) -> int:
+        return int(ffi.cast("uintptr_t", lib.mm_plan_device_output(self._plan)))
+
+    @property
+    def device_mel_db(self) -> int:
+        return int(ffi.cast("uintptr_t", lib.mm_plan_device_mel_db(self._plan)))
+
+    def clip_max_db(self, clip: int) -> float:
+        v = ffi.new("float*")
+        st = lib.mm_plan_clip_max_db(self._plan, clip, v)
+        if st != 0:
+            raise RuntimeError(f"mm_plan_clip_max_db failed with status {st}")
+        return float(v[0])
+
+    def execute(self, stream: int = 0):
+        st = lib.mm_plan_execute(self._plan, ffi.cast("void*", stream))
+        if st != 0:
+            raise RuntimeError(f"mm_plan_execute failed with status {st}")
+
+    def execute_timed(self, slot: int, stream: int = 0):
+        st = lib.mm_plan_execute_timed(self._plan, ffi.cast("void*", stream), slot)
+        if st != 0:
+            raise RuntimeError(f"mm_plan_execute_timed failed with status {st}")
+
+    def stage_ms(self, slot: int):
+        ms = ffi.new("float[3]")
+        st = lib.mm_plan_stage_ms(self._plan, slot, ms)
+        if st != 0:
+            raise RuntimeError(f"mm_plan_stage_ms failed with status {st}")
+        return [ms[0], ms[1], ms[2]]
+
+    def alloc_outputs(self):
+        return [np.empty((self.rows, f), dtype=np.float32) for f in self.frames]
+
+    def execute_host(self, clips, outs=None, stream: int = 0):
+        """Copy ``clips`` in, run, copy MFCCs out (into ``outs`` if given)."""
+        clips = [np.ascontiguousarray(c, dtype=np.float32) for c in clips]
+        if len(clips) != self.n or any(len(c) != L for c, L in zip(clips, self.lengths)):
+            raise ValueError("clips do not match the plan's lengths")
+        if outs is None:
+            outs = self.alloc_outputs()
+        ins = ffi.new("const float*[]", [ffi.cast("const float*", c.ctypes.data) for c in clips])
+        ops = ffi.new("float*[]", [ffi.cast("float*", o.ctypes.data) for o in outs])
+        st = lib.mm_plan_execute_host(self._plan, ins, ops, ffi.cast("void*", stream))
+        if st != 0:
+            raise RuntimeError(f"mm_plan_execute_host failed with status {st}")
+        return outs
+
+    def close(self):
+        if getattr(self, "_plan", None) is not None and self._plan != ffi.NULL:
+            lib.mm_plan_destroy(self._plan)
+            lib.mm_destroy(self._ctx)
+        self._plan = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,455 @@
+// extern "C" entry points of libmetalmom.so (declared in include/metalmom.h).
+//
+// The reference entry points keep MetalMom's validation order, sentinels,
+// status codes, output shapes and ownership rules (Bridge.swift:16-492,
+// 3695-3711); the work itself runs on the CUDA device.
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <unordered_set>
+#include <vector>
+
+#include "runtime.h"
+
+using namespace mm;
+
+namespace {
+
+// Context registry: makes mm_destroy idempotent (Bridge.swift:16-40).
+struct Context {
+  int magic = 0x4d4d4232;
+};
+std::mutex g_ctx_mu;
+std::unordered_set<void *> g_ctx;
+
+// Run one clip (n = 1) or a batch of clips through `g`; on success *outs[i]
+// holds a malloc'd [rows x n_frames_i] block (NULL when empty).
+int run_batch(const Group &g, const float *const *signals, const int64_t *lengths, int n,
+              float **outs) {
+  for (int i = 0; i < n; i++) outs[i] = nullptr;
+  Layout L;
+  make_layout(g, lengths, n, L);
+  if (L.total_frames == 0 || L.out_elems == 0) return MM_OK;
+  int st = gpu_available();
+  if (st != MM_OK) return st;
+  const DevTables *t = get_tables(g, &st);
+  if (!t) return st;
+  const size_t dev_bytes = arena_bytes(g, L);
+  DevBatch probe;
+  const size_t desc_bytes = carve_arena(g, L, nullptr, probe);
+  const size_t sig_bytes = sizeof(float) * (size_t)L.sig_elems;
+  const size_t out_bytes = sizeof(float) * (size_t)L.out_elems;
+  const size_t host_bytes = std::max(sig_bytes + desc_bytes, out_bytes) + 256;
+  Workspace *ws = nullptr;
+  if ((st = thread_workspace(dev_bytes, host_bytes, &ws)) != MM_OK) return st;
+  DevBatch b;
+  carve_arena(g, L, ws->dev, b);
+  cudaStream_t s = ws->stream;
+  cudaError_t e = cudaStreamSynchronize(s);  // staging buffer is free again
+  if (e != cudaSuccess) return cuda_status(e);
+  // Stage signals + descriptors in pinned memory, then one async copy each.
+  char *h = ws->host;
+  for (int i = 0; i < n; i++)
+    memcpy(h + sizeof(float) * (size_t)L.clips[i].sig_off, signals[i], sizeof(float) * (size_t)lengths[i]);
+  pack_descriptors(L, h + sig_bytes);
+  if ((e = cudaMemcpyAsync(b.signal, h, sig_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = cudaMemcpyAsync(b.clips, h + sig_bytes, desc_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = enqueue_batch(g, L, t, b, s, nullptr, nullptr)) != cudaSuccess) return cuda_status(e);
+  if ((e = cudaMemcpyAsync(h, b.out, out_bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e);
+  const int rows = output_rows(g);
+  for (int i = 0; i < n; i++) {
+    const size_t cnt = (size_t)rows * (size_t)L.clips[i].n_frames;
+    if (cnt == 0) continue;
+    outs[i] = (float *)malloc(sizeof(float) * cnt);
+    if (!outs[i]) {
+      for (int q = 0; q < i; q++) free(outs[q]), outs[q] = nullptr;
+      return MM_ERR_ALLOC_FAILED;
+    }
+    memcpy(outs[i], h + sizeof(float) * (size_t)L.clips[i].out_off, sizeof(float) * cnt);
+  }
+  return MM_OK;
+}
+
+// Resolve the mel / MFCC sentinels (Bridge.swift:340-345, 432-437).
+int resolve_mel_group(Group &g, int sr, int n_fft, int hop, int win, int center, int n_mels,
+                      float fmin, float fmax) {
+  if (n_fft <= 0 || n_mels < 0) return MM_ERR_INVALID_INPUT;
+  g.sr = sr;
+  g.n_fft = n_fft;
+  g.log2n = ilog2(n_fft);
+  g.hop = hop > 0 ? hop : n_fft / 4;
+  g.win = win > 0 ? win : n_fft;
+  g.window_zero = 0;
+  g.center = center != 0;
+  g.pad_mode = PAD_CONSTANT;
+  g.n_mels = n_mels;
+  g.fmin = fmin;
+  g.fmax = fmax > 0.0f ? fmax : (float)sr / 2.0f;
+  if (g.hop <= 0) return MM_ERR_INVALID_INPUT;  // the reference divides by zero here
+  return MM_OK;
+}
+
+bool supported_size(const Group &g) { return g.log2n <= 15; }
+
+}  // namespace
+
+extern "C" {
+
+mm_context mm_init(void) {
+  Context *c = new (std::nothrow) Context();
+  if (!c) return nullptr;
+  std::lock_guard<std::mutex> lock(g_ctx_mu);
+  g_ctx.insert(c);
+  return c;
+}
+
+void mm_destroy(mm_context ctx) {
+  if (!ctx) return;
+  {
+    std::lock_guard<std::mutex> lock(g_ctx_mu);
+    if (g_ctx.erase(ctx) == 0) return;  // already destroyed
+  }
+  delete static_cast<Context *>(ctx);
+}
+
+void mm_buffer_free(MMBuffer *buf) {
+  if (!buf) return;
+  free(buf->data);
+  buf->data = nullptr;
+  buf->ndim = 0;
+  buf->dtype = 0;
+  buf->count = 0;
+  for (int i = 0; i < 8; i++) buf->shape[i] = 0;
+}
+
+int32_t mm_stft(mm_context ctx, const float *signal_data, int64_t signal_length, int32_t sample_rate,
+                const MMSTFTParams *params, MMBuffer *out) {
+  if (!ctx || !signal_data || signal_length <= 0 || !params || !out) return MM_ERR_INVALID_INPUT;
+  const int n_fft = params->n_fft;
+  if (!is_pow2(n_fft)) return MM_ERR_INVALID_INPUT;
+  Group g;
+  g.mode = MODE_SPECTRUM;
+  g.power = 1.0f;
+  g.sr = sample_rate;
+  g.n_fft = n_fft;
+  g.log2n = ilog2(n_fft);
+  g.hop = params->hop_length;
+  g.win = params->win_length;
+  g.window_zero = params->win_length <= 0;
+  g.center = params->center != 0;
+  g.n_mels = 0;
+  g.n_mfcc_eff = 0;
+  if (g.hop <= 0 || !supported_size(g)) return MM_ERR_INVALID_INPUT;
+  const long long T = frame_count(signal_length, n_fft, g.hop, g.center);
+  const long long rows = n_fft / 2 + 1;
+  float *data = nullptr;
+  if (T > 0) {
+    int st = run_batch(g, &signal_data, &signal_length, 1, &data);
+    if (st != MM_OK) return st;
+  }
+  fill_buffer(out, data, rows, T);
+  return MM_OK;
+}
+
+static int32_t db_common(const float *data, int64_t count, float mult, float ref, float amin,
+                         float top_db, MMBuffer *out) {
+  if (!data || count <= 0 || !out) return MM_ERR_INVALID_INPUT;
+  int st = gpu_available();
+  if (st != MM_OK) return st;
+  const size_t bytes = sizeof(float) * (size_t)count;
+  const size_t seg = ((bytes + 255) / 256) * 256;
+  Workspace *ws = nullptr;
+  if ((st = thread_workspace(2 * seg + 256, bytes, &ws)) != MM_OK) return st;
+  cudaStream_t s = ws->stream;
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e);
+  float *d_x = reinterpret_cast<float *>(ws->dev);
+  float *d_y = reinterpret_cast<float *>(ws->dev + seg);
+  unsigned *slot = reinterpret_cast<unsigned *>(ws->dev + 2 * seg);
+  memcpy(ws->host, data, bytes);
+  if ((e = cudaMemcpyAsync(d_x, ws->host, bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = launch_db(d_x, d_y, count, mult, amin, ref, top_db, slot, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = cudaMemcpyAsync(ws->host, d_y, bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_status(e);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e);
+  float *res = (float *)malloc(bytes);
+  if (!res) return MM_ERR_ALLOC_FAILED;
+  memcpy(res, ws->host, bytes);
+  fill_buffer(out, res, count, 0);
+  out->ndim = 1;
+  out->shape[1] = 0;
+  out->count = count;
+  return MM_OK;
+}
+
+int32_t mm_power_to_db(mm_context ctx, const float *data, int64_t count, float ref, float amin,
+                       float top_db, MMBuffer *out) {
+  (void)ctx;  // the reference does not check the context here (Bridge.swift:276-278)
+  return db_common(data, count, 10.0f, ref, amin, top_db, out);
+}
+
+int32_t mm_amplitude_to_db(mm_context ctx, const float *data, int64_t count, float ref, float amin,
+                           float top_db, MMBuffer *out) {
+  (void)ctx;
+  return db_common(data, count, 20.0f, ref, amin, top_db, out);
+}
+
+int32_t mm_mel_spectrogram(mm_context ctx, const float *signal_data, int64_t signal_length,
+                           int32_t sample_rate, int32_t n_fft, int32_t hop_length, int32_t win_length,
+                           int32_t center, float power, int32_t n_mels, float f_min, float f_max,
+                           MMBuffer *out) {
+  if (!ctx || !signal_data || signal_length <= 0 || !out) return MM_ERR_INVALID_INPUT;
+  Group g;
+  int st = resolve_mel_group(g, sample_rate, n_fft, hop_length, win_length, center, n_mels, f_min, f_max);
+  if (st != MM_OK) return st;
+  g.mode = MODE_MEL;
+  g.power = power;
+  g.n_mfcc_eff = 0;
+  const long long T = frame_count(signal_length, g.n_fft, g.hop, g.center);
+  float *data = nullptr;
+  if (T > 0 && n_mels > 0) {
+    if (!supported_size(g)) return MM_ERR_INVALID_INPUT;
+    st = run_batch(g, &signal_data, &signal_length, 1, &data);
+    if (st != MM_OK) return st;
+  }
+  fill_buffer(out, data, n_mels, T);
+  return MM_OK;
+}
+
+int32_t mm_mfcc(mm_context ctx, const float *signal_data, int64_t signal_length, int32_t sample_rate,
+                int32_t n_mfcc, int32_t n_fft, int32_t hop_length, int32_t win_length, int32_t n_mels,
+                float f_min, float f_max, int32_t center, MMBuffer *out) {
+  if (!ctx || !signal_data || signal_length <= 0 || !out) return MM_ERR_INVALID_INPUT;
+  Group g;
+  int st = resolve_mel_group(g, sample_rate, n_fft, hop_length, win_length, center, n_mels, f_min, f_max);
+  if (st != MM_OK) return st;
+  if (n_mfcc < 0) return MM_ERR_INVALID_INPUT;
+  g.mode = MODE_MELDB;
+  g.power = 2.0f;
+  g.amin = 1e-10f;
+  g.ref = 1.0f;
+  g.top_db = 80.0f;
+  g.n_mfcc_eff = std::min(n_mfcc, n_mels);
+  const long long T = frame_count(signal_length, g.n_fft, g.hop, g.center);
+  float *data = nullptr;
+  if (T > 0 && g.n_mfcc_eff > 0) {
+    if (!supported_size(g)) return MM_ERR_INVALID_INPUT;
+    st = run_batch(g, &signal_data, &signal_length, 1, &data);
+    if (st != MM_OK) return st;
+  }
+  fill_buffer(out, data, g.n_mfcc_eff, T);
+  return MM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// additive: batches and plans
+// ---------------------------------------------------------------------------
+static int resolve_frontend(const MMFrontEndParams *p, Group &g) {
+  if (!p) return MM_ERR_INVALID_INPUT;
+  int st = resolve_mel_group(g, p->sample_rate, p->n_fft, p->hop_length, p->win_length, p->center,
+                             p->n_mels, p->f_min, p->f_max);
+  if (st != MM_OK) return st;
+  if (p->n_mfcc < 0 || (p->pad_mode != MM_PAD_CONSTANT && p->pad_mode != MM_PAD_REFLECT))
+    return MM_ERR_INVALID_INPUT;
+  if (!is_pow2(p->n_fft) || !supported_size(g)) return MM_ERR_INVALID_INPUT;
+  g.mode = MODE_MELDB;
+  g.pad_mode = p->pad_mode;
+  g.power = 2.0f;
+  g.amin = 1e-10f;
+  g.ref = 1.0f;
+  g.top_db = p->top_db;
+  g.n_mfcc_eff = std::min(p->n_mfcc, p->n_mels);
+  return MM_OK;
+}
+
+int32_t mm_mfcc_batch(mm_context ctx, const float *const *signals, const int64_t *lengths,
+                      int32_t n_clips, const MMFrontEndParams *params, MMBuffer *outs) {
+  if (!ctx || !signals || !lengths || n_clips <= 0 || !outs) return MM_ERR_INVALID_INPUT;
+  for (int i = 0; i < n_clips; i++)
+    if (!signals[i] || lengths[i] <= 0) return MM_ERR_INVALID_INPUT;
+  Group g;
+  int st = resolve_frontend(params, g);
+  if (st != MM_OK) return st;
+  std::vector<float *> data(n_clips, nullptr);
+  if (g.n_mfcc_eff > 0) {
+    st = run_batch(g, signals, lengths, n_clips, data.data());
+    if (st != MM_OK) return st;
+  }
+  for (int i = 0; i < n_clips; i++)
+    fill_buffer(&outs[i], data[i], g.n_mfcc_eff, frame_count(lengths[i], g.n_fft, g.hop, g.center));
+  return MM_OK;
+}
+
+namespace {
+constexpr int kSlots = 64;
+struct Plan {
+  Group g;
+  Layout L;
+  const DevTables *t = nullptr;
+  char *arena = nullptr;
+  DevBatch b;
+  cudaStream_t stream = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[kSlots][4] = {};
+  int launches = 0;
+  int device = 0;
+};
+
+void plan_free(Plan *p) {
+  if (!p) return;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  for (int s = 0; s < kSlots; s++)
+    for (int q = 0; q < 4; q++)
+      if (p->ev[s][q]) cudaEventDestroy(p->ev[s][q]);
+  if (p->arena) cudaFree(p->arena);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+}
+}  // namespace
+
+mm_plan mm_plan_create(mm_context ctx, const MMFrontEndParams *params, const int64_t *lengths,
+                       int32_t n_clips, int32_t *status) {
+  int dummy;
+  int32_t *st_out = status ? status : &dummy;
+  *st_out = MM_ERR_INVALID_INPUT;
+  if (!ctx || !lengths || n_clips <= 0) return nullptr;
+  for (int i = 0; i < n_clips; i++)
+    if (lengths[i] <= 0) return nullptr;
+  Plan *p = new (std::nothrow) Plan();
+  if (!p) {
+    *st_out = MM_ERR_ALLOC_FAILED;
+    return nullptr;
+  }
+  int st = resolve_frontend(params, p->g);
+  if (st == MM_OK) st = gpu_available();
+  if (st == MM_OK) p->t = get_tables(p->g, &st);
+  if (st != MM_OK) {
+    *st_out = st;
+    delete p;
+    return nullptr;
+  }
+  cudaGetDevice(&p->device);
+  make_layout(p->g, lengths, n_clips, p->L);
+  cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&p->arena, arena_bytes(p->g, p->L));
+  if (e == cudaSuccess) {
+    const size_t desc = carve_arena(p->g, p->L, p->arena, p->b);
+    std::vector<char> host(desc + 16);
+    pack_descriptors(p->L, host.data());
+    e = cudaMemsetAsync(p->arena, 0, sizeof(float) * (size_t)p->L.sig_elems, p->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p->b.clips, host.data(), desc, cudaMemcpyHostToDevice, p->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+  }
+  for (int s = 0; s < kSlots && e == cudaSuccess; s++)
+    for (int q = 0; q < 4 && e == cudaSuccess; q++) e = cudaEventCreate(&p->ev[s][q]);
+  if (e == cudaSuccess) e = cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed);
+  if (e == cudaSuccess) {
+    cudaError_t e1 = enqueue_batch(p->g, p->L, p->t, p->b, p->stream, nullptr, &p->launches);
+    cudaError_t e2 = cudaStreamEndCapture(p->stream, &p->graph);
+    e = (e1 != cudaSuccess) ? e1 : e2;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *st_out = cuda_status(e);
+    plan_free(p);
+    return nullptr;
+  }
+  *st_out = MM_OK;
+  return p;
+}
+
+void mm_plan_destroy(mm_plan plan) { plan_free(static_cast<Plan *>(plan)); }
+
+float *mm_plan_device_input(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.signal : nullptr; }
+float *mm_plan_device_output(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.out : nullptr; }
+
+int64_t mm_plan_input_offset(mm_plan plan, int32_t clip) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
+  return p->L.clips[clip].sig_off;
+}
+int64_t mm_plan_output_offset(mm_plan plan, int32_t clip) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
+  return p->L.clips[clip].out_off;
+}
+int64_t mm_plan_clip_frames(mm_plan plan, int32_t clip) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
+  return p->L.clips[clip].n_frames;
+}
+int32_t mm_plan_rows(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->g.n_mfcc_eff : -1; }
+int64_t mm_plan_total_frames(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->L.total_frames : -1; }
+int32_t mm_plan_kernel_launches(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->launches : -1; }
+
+float *mm_plan_device_mel_db(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.meldb : nullptr; }
+
+int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float *max_db) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || clip < 0 || clip >= (int)p->L.clips.size() || !max_db) return MM_ERR_INVALID_INPUT;
+  unsigned u = 0;
+  cudaError_t e = cudaMemcpy(&u, p->b.clip_max + clip, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e);
+  *max_db = decode_max(u);
+  return MM_OK;
+}
+
+int32_t mm_plan_execute(mm_plan plan, void *stream) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p) return MM_ERR_INVALID_INPUT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+  return cuda_status(cudaGraphLaunch(p->exec, s));
+}
+
+int32_t mm_plan_execute_timed(mm_plan plan, void *stream, int32_t slot) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || slot < 0 || slot >= kSlots) return MM_ERR_INVALID_INPUT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+  return cuda_status(enqueue_batch(p->g, p->L, p->t, p->b, s, p->ev[slot], nullptr));
+}
+
+int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float *ms3) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || slot < 0 || slot >= kSlots || !ms3) return MM_ERR_INVALID_INPUT;
+  for (int q = 0; q < 3; q++) {
+    cudaError_t e = cudaEventElapsedTime(&ms3[q], p->ev[slot][q], p->ev[slot][q + 1]);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  return MM_OK;
+}
+
+int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *const *outs, void *stream) {
+  Plan *p = static_cast<Plan *>(plan);
+  if (!p || !signals || !outs) return MM_ERR_INVALID_INPUT;
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
+  cudaError_t e = cudaSuccess;
+  const int n = (int)p->L.clips.size();
+  for (int i = 0; i < n && e == cudaSuccess; i++) {
+    const ClipDesc &c = p->L.clips[i];
+    e = cudaMemcpyAsync(p->b.signal + c.sig_off, signals[i], sizeof(float) * (size_t)c.length,
+                        cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, s);
+  const int rows = p->g.n_mfcc_eff;
+  for (int i = 0; i < n && e == cudaSuccess; i++) {
+    const ClipDesc &c = p->L.clips[i];
+    const size_t cnt = (size_t)rows * (size_t)c.n_frames;
+    if (cnt) e = cudaMemcpyAsync(outs[i], p->b.out + c.out_off, sizeof(float) * cnt, cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return cuda_status(e);
+}
+
+}  // extern "C"

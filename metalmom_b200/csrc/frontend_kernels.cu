@@ -1,0 +1,773 @@
+// Frame kernels for the spectral front end on sm_100a.
+//
+// One CTA tile = F consecutive frames of one clip.  Per frame:
+//   gather + window (float2 loads straight from HBM, padding handled in the
+//   index math) -> complex FFT of n_fft/2 points (Stockham, radix-16 stages in
+//   registers, exchanges through bank-padded shared memory) -> real split ->
+//   |X|^2 -> mode epilogue (spectrum rows, mel rows, or log-mel + per-clip max).
+// A second kernel applies the clip-global top_db floor and the DCT-II.
+//
+// Reference semantics followed (MetalMom, Sources/MetalMomCore):
+//   frame count / zero padding   Spectral/STFT.swift:241-254
+//   window placement             Spectral/STFT.swift:44-57, Filters/Windows.swift:14-48
+//   DFT scaling (plain DFT)      Spectral/STFT.swift:298-329
+//   dense mel product            Spectral/MelSpectrogram.swift:127-138
+//   power_to_db + top_db         Spectral/Scaling.swift:73-118
+//   DCT-II ortho                 Features/MFCC.swift:65-106
+#include <math.h>
+#include <string.h>
+
+#include "fft_radix.cuh"
+#include "kernels.h"
+
+namespace mm {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+
+// Order-preserving float -> uint map so atomicMax on uint is a float max.
+__host__ __device__ __forceinline__ unsigned enc_f(float f) {
+  unsigned b;
+#ifdef __CUDA_ARCH__
+  b = __float_as_uint(f);
+#else
+  memcpy(&b, &f, 4);
+#endif
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float dec_f(unsigned u) {
+  unsigned b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  return __uint_as_float(b);
+}
+unsigned encode_max_init() { return enc_f(-INFINITY); }
+float decode_max(unsigned u) {
+  unsigned b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+// vDSP_vthr: x if x >= t else t (a NaN x becomes t).
+__device__ __forceinline__ float vthr(float x, float t) { return x >= t ? x : t; }
+
+__device__ __forceinline__ float apply_power(float pw, float power) {
+  if (power == 2.0f) return pw;
+  float mag = sqrtf(pw);
+  if (power == 1.0f) return mag;
+  return powf(mag, power);
+}
+
+__device__ __forceinline__ long long reflect_idx(long long i, long long L) {
+  if (L <= 1) return 0;
+  long long period = 2 * (L - 1);
+  long long m = i % period;
+  if (m < 0) m += period;
+  return m < L ? m : period - m;
+}
+
+__device__ __forceinline__ float sample_at(const float *sig, long long i, long long L, int pad_mode) {
+  if (i >= 0 && i < L) return __ldg(sig + i);
+  if (pad_mode == PAD_REFLECT) return __ldg(sig + reflect_idx(i, L));
+  return 0.0f;
+}
+
+__device__ __forceinline__ int padx(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ ClipDesc load_clip(const ClipDesc *p) {
+  ClipDesc d;
+  d.sig_off = __ldg(&p->sig_off);
+  d.length = __ldg(&p->length);
+  d.frame_off = __ldg(&p->frame_off);
+  d.out_off = __ldg(&p->out_off);
+  d.n_frames = __ldg(&p->n_frames);
+  d.tile_base = __ldg(&p->tile_base);
+  return d;
+}
+
+__device__ __forceinline__ cpx ldc(const float2 *p) {
+  float2 v = __ldg(p);
+  return {v.x, v.y};
+}
+
+// ---------------------------------------------------------------------------
+// FFT shape for a real frame of N = 2^LOG2N samples (complex length M = N/2):
+// radix-16 stages followed by one radix-RLAST stage when log2(M) % 4 != 0.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int stage_radix(int log2m, int q) { return q < log2m / 4 ? 16 : (1 << (log2m % 4)); }
+__host__ __device__ constexpr int stage_ns(int log2m, int q) {
+  int ns = 1;
+  for (int i = 0; i < q; i++) ns *= stage_radix(log2m, i);
+  return ns;
+}
+// Offset of stage q's twiddles {W_{R*Ns}^(k*r) : r in [1,R), k in [0,Ns)}, stored [r-1][k].
+__host__ __device__ constexpr int stage_tw_off(int log2m, int q) {
+  int off = 0;
+  for (int i = 1; i < q; i++) off += (stage_radix(log2m, i) - 1) * stage_ns(log2m, i);
+  return off;
+}
+__host__ __device__ constexpr int n_stages(int log2m) { return log2m / 4 + ((log2m % 4) ? 1 : 0); }
+__host__ __device__ constexpr int tw_count(int log2m) { return stage_tw_off(log2m, n_stages(log2m)); }
+
+template <int LOG2N>
+struct Shape {
+  static constexpr int N = 1 << LOG2N;
+  static constexpr int M = N / 2;
+  static constexpr int LOG2M = LOG2N - 1;
+  static constexpr int TPF = M / 16;  // threads per frame
+  static constexpr int N16 = LOG2M / 4;
+  static constexpr int RLAST = 1 << (LOG2M % 4);
+  static constexpr int PADM = M + M / 16;
+  static constexpr int FSTRIDE = PADM + 1;  // complex slots per frame (odd: spreads banks)
+  static constexpr bool TW_SMEM = (M <= 4096);
+  static constexpr int TWC = tw_count(LOG2M);
+  static constexpr int TWN = M / 2;
+};
+
+int stage_twiddle_count(int log2n) { return log2n >= 5 ? tw_count(log2n - 1) : 0; }
+
+int frames_per_tile(int log2n) {
+  switch (log2n) {
+    case 5: return 128;
+    case 6: return 64;
+    case 7: return 32;
+    case 8: return 32;
+    case 9: return 16;
+    case 10: return 8;
+    case 11: return 4;
+    case 12: return 2;
+    case 13: case 14: case 15: return 1;
+    default: return 128;  // tiny kernel (n_fft <= 16)
+  }
+}
+
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
+
+template <int LOG2N, int F>
+__host__ __device__ constexpr size_t fixed_smem_bytes() {
+  using S = Shape<LOG2N>;
+  return 128 + align16(F * 4) +
+         (S::TW_SMEM ? align16(size_t(S::TWC) * 8) + align16(size_t(S::TWN) * 8) : 0) +
+         size_t(F) * S::FSTRIDE * 8;
+}
+
+// ---------------------------------------------------------------------------
+// epilogue (shared by the FFT kernels): P holds |X|^power for F frames
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float mel_dot(int4 info, const float *__restrict__ w, const float *P,
+                                         bool bad) {
+  const float *wr = w + info.z;
+  const float *pr = P + info.x;
+  float acc = 0.0f;
+  for (int q = 0; q < info.y; q++) acc = fmaf(__ldg(wr + q), pr[q], acc);
+  if (info.w || bad) acc = __int_as_float(0x7fc00000);
+  return acc;
+}
+
+template <int MODE, int F, int THREADS>
+__device__ __forceinline__ void epilogue(const FrontArgs &a, const float *P0, int fstride, int nfreq,
+                                         const int *bad_s, const ClipDesc &cd, int c, int t0,
+                                         const int4 *mel_s, float *red_s) {
+  const int tid = threadIdx.x;
+  const long long T = cd.n_frames;
+  if constexpr (MODE == MODE_SPECTRUM) {
+    for (int it = tid; it < F * nfreq; it += THREADS) {
+      const int fi = it % F, k = it / F;
+      const int t = t0 + fi;
+      if (t < cd.n_frames) a.out[cd.out_off + (long long)k * T + t] = P0[fi * fstride + k];
+    }
+  } else if constexpr (MODE == MODE_MEL) {
+    for (int it = tid; it < F * a.n_mels; it += THREADS) {
+      const int fi = it % F, m = it / F;
+      const int t = t0 + fi;
+      if (t >= cd.n_frames) continue;
+      float acc = mel_dot(mel_s[m], a.mel_w, P0 + fi * fstride, bad_s[fi] != 0);
+      a.out[cd.out_off + (long long)m * T + t] = acc;
+    }
+  } else {
+    float vmax = -INFINITY;
+    for (int it = tid; it < F * a.n_mels; it += THREADS) {
+      const int fi = it / a.n_mels, m = it - fi * a.n_mels;
+      const int t = t0 + fi;
+      if (t >= cd.n_frames) continue;
+      float acc = mel_dot(mel_s[m], a.mel_w, P0 + fi * fstride, bad_s[fi] != 0);
+      float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+      a.out[(cd.frame_off + t) * (long long)a.n_mels + m] = v;
+      vmax = fmaxf(vmax, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    if ((tid & 31) == 0) red_s[tid >> 5] = vmax;
+    __syncthreads();
+    if (tid < 32) {
+      float v = (tid < (THREADS + 31) / 32) ? red_s[tid] : -INFINITY;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if (tid == 0 && v > -INFINITY) atomicMax(a.clip_max + c, enc_f(v));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// main frame kernel, n_fft = 2^LOG2N with LOG2N in [5, 15]
+// ---------------------------------------------------------------------------
+template <int LOG2N, int F, int MODE>
+__global__ void __launch_bounds__(Shape<LOG2N>::TPF * F, (1024 / (Shape<LOG2N>::TPF * F)) > 0 ? (1024 / (Shape<LOG2N>::TPF * F)) : 1)
+frontend_kernel(FrontArgs a) {
+  using S = Shape<LOG2N>;
+  constexpr int N = S::N, M = S::M, TPF = S::TPF, THREADS = TPF * F;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nmel_s = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  unsigned char *sp = smem;
+  int4 *mel_s = reinterpret_cast<int4 *>(sp);
+  sp += 16 * (size_t)nmel_s;
+  float *red_s = reinterpret_cast<float *>(sp);
+  sp += 128;
+  int *bad_s = reinterpret_cast<int *>(sp);
+  sp += align16(F * 4);
+  cpx *tws_s = reinterpret_cast<cpx *>(sp);
+  if constexpr (S::TW_SMEM) sp += align16(size_t(S::TWC) * 8);
+  cpx *twn_s = reinterpret_cast<cpx *>(sp);
+  if constexpr (S::TW_SMEM) sp += align16(size_t(S::TWN) * 8);
+  cpx *buf = reinterpret_cast<cpx *>(sp);
+
+  const int tid = threadIdx.x;
+  const int f = tid / TPF;
+  const int j = tid - f * TPF;
+
+  if constexpr (S::TW_SMEM) {
+    for (int i = tid; i < S::TWC; i += THREADS) tws_s[i] = ldc(a.tw_stage + i);
+    for (int i = tid; i < S::TWN; i += THREADS) twn_s[i] = ldc(a.tw_split + i);
+  }
+  for (int i = tid; i < nmel_s; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  const cpx *tws = S::TW_SMEM ? tws_s : reinterpret_cast<const cpx *>(a.tw_stage);
+  const cpx *twn = S::TW_SMEM ? twn_s : reinterpret_cast<const cpx *>(a.tw_split);
+  __syncthreads();
+
+  cpx *fb = buf + f * S::FSTRIDE;
+
+  for (int tile = blockIdx.x; tile < a.total_tiles; tile += gridDim.x) {
+    const int c = __ldg(a.tile_clip + tile);
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int t0 = (tile - cd.tile_base) * F;
+    const long long s0 = (long long)(t0 + f) * a.hop - a.pad;
+    const float *sig = a.signal + cd.sig_off;
+
+    // ---- gather: z[n] = (x[2n] w[2n], x[2n+1] w[2n+1]) for n = j + r*M/16
+    cpx v[16];
+    if (s0 >= 0 && s0 + N <= cd.length) {
+      const float *base = sig + s0 + 2 * j;
+      const float *wb = a.window + 2 * j;
+      if (((cd.sig_off + s0) & 1) == 0) {
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+          const float2 x = __ldg(reinterpret_cast<const float2 *>(base + r * (N / 16)));
+          const float2 w = __ldg(reinterpret_cast<const float2 *>(wb + r * (N / 16)));
+          v[r] = {x.x * w.x, x.y * w.y};
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+          const float2 w = __ldg(reinterpret_cast<const float2 *>(wb + r * (N / 16)));
+          v[r] = {__ldg(base + r * (N / 16)) * w.x, __ldg(base + r * (N / 16) + 1) * w.y};
+        }
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 16; r++) {
+        const int n0 = 2 * j + r * (N / 16);
+        const float2 w = __ldg(reinterpret_cast<const float2 *>(a.window + n0));
+        v[r] = {sample_at(sig, s0 + n0, cd.length, a.pad_mode) * w.x,
+                sample_at(sig, s0 + n0 + 1, cd.length, a.pad_mode) * w.y};
+      }
+    }
+
+    // ---- stage 0: radix 16, Ns = 1 (no twiddles)
+    dft16(v);
+    __syncthreads();  // the previous tile's epilogue has finished with buf / bad_s
+    if (j == 0) bad_s[f] = 0;
+#pragma unroll
+    for (int r = 0; r < 16; r++) fb[padx(j * 16 + r)] = v[r];
+    __syncthreads();
+
+    // ---- radix-16 stages 1 .. N16-1
+#pragma unroll
+    for (int q = 1; q < S::N16; q++) {
+      const int Ns = 1 << (4 * q);
+      const int k = j & (Ns - 1);
+      const cpx *tw = tws + stage_tw_off(S::LOG2M, q) + k;
+#pragma unroll
+      for (int r = 0; r < 16; r++) v[r] = fb[padx(j + r * (M / 16))];
+#pragma unroll
+      for (int r = 1; r < 16; r++) v[r] = cmul(v[r], tw[(r - 1) * Ns]);
+      dft16(v);
+      __syncthreads();
+      const int base = (j - k) * 16 + k;
+#pragma unroll
+      for (int r = 0; r < 16; r++) fb[padx(base + r * Ns)] = v[r];
+      __syncthreads();
+    }
+
+    // ---- trailing radix-R stage (in place: each thread rewrites what it read)
+    if constexpr (S::RLAST > 1) {
+      constexpr int R = S::RLAST, B = 16 / R, Ns = M / R;
+      const cpx *tw = tws + stage_tw_off(S::LOG2M, S::N16);
+#pragma unroll
+      for (int i = 0; i < B; i++) {
+        const int b = j + i * TPF;
+#pragma unroll
+        for (int qq = 0; qq < R; qq++) v[i * R + qq] = fb[padx(b + qq * Ns)];
+#pragma unroll
+        for (int qq = 1; qq < R; qq++) v[i * R + qq] = cmul(v[i * R + qq], tw[(qq - 1) * Ns + b]);
+        dft<R>(v + i * R);
+#pragma unroll
+        for (int qq = 0; qq < R; qq++) fb[padx(b + qq * Ns)] = v[i * R + qq];
+      }
+      __syncthreads();
+    }
+
+    // ---- real split: X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
+    float pa[8], pb[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int k = j + i * TPF;
+      if (k == 0) {
+        const cpx z = fb[0];
+        const float dc = z.x + z.y, ny = z.x - z.y;
+        pa[i] = dc * dc;
+        pb[i] = ny * ny;
+      } else {
+        const cpx za = fb[padx(k)], zb = fb[padx(M - k)];
+        const cpx E = {0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y)};
+        const cpx O = {0.5f * (za.y + zb.y), -0.5f * (za.x - zb.x)};
+        const cpx WO = cmul(twn[k], O);
+        const float xr = E.x + WO.x, xi = E.y + WO.y;
+        const float yr = E.x - WO.x, yi = E.y - WO.y;
+        pa[i] = xr * xr + xi * xi;
+        pb[i] = yr * yr + yi * yi;
+      }
+    }
+    float pmid = 0.0f;
+    if (j == 0) {
+      const cpx z = fb[padx(M / 2)];
+      pmid = z.x * z.x + z.y * z.y;
+    }
+    __syncthreads();
+    float *P = reinterpret_cast<float *>(fb);
+    bool nonfinite = false;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int k = j + i * TPF;
+      const float x = apply_power(pa[i], a.power);
+      const float y = apply_power(pb[i], a.power);
+      P[k] = x;
+      P[M - k] = y;
+      nonfinite |= !(isfinite(x) && isfinite(y));
+    }
+    if (j == 0) {
+      const float x = apply_power(pmid, a.power);
+      P[M / 2] = x;
+      nonfinite |= !isfinite(x);
+    }
+    if (MODE != MODE_SPECTRUM && nonfinite) bad_s[f] = 1;
+    __syncthreads();
+
+    epilogue<MODE, F, THREADS>(a, reinterpret_cast<const float *>(buf), 2 * S::FSTRIDE, M + 1,
+                               bad_s, cd, c, t0, mel_s, red_s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tiny frames (n_fft <= 16): direct DFT, one thread per frame
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_fft) {
+  constexpr int F = 128, THREADS = 128, PST = 9;
+  __shared__ float P_s[F * PST];
+  __shared__ int bad_s[F];
+  __shared__ float red_s[32];
+  extern __shared__ __align__(16) unsigned char smem[];
+  int4 *mel_s = reinterpret_cast<int4 *>(smem);
+  const int nmel_s = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < nmel_s; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  const int nfreq = n_fft / 2 + 1;
+  for (int tile = blockIdx.x; tile < a.total_tiles; tile += gridDim.x) {
+    const int c = __ldg(a.tile_clip + tile);
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int t0 = (tile - cd.tile_base) * F;
+    const long long s0 = (long long)(t0 + tid) * a.hop - a.pad;
+    const float *sig = a.signal + cd.sig_off;
+    float xw[16];
+#pragma unroll
+    for (int n = 0; n < 16; n++)
+      xw[n] = (n < n_fft) ? sample_at(sig, s0 + n, cd.length, a.pad_mode) * __ldg(a.window + n) : 0.0f;
+    float p[PST];
+    bool nonfinite = false;
+#pragma unroll
+    for (int k = 0; k < PST; k++) {
+      float re = 0.0f, im = 0.0f;
+      if (k < nfreq) {
+        for (int n = 0; n < n_fft; n++) {
+          const float2 w = __ldg(a.tw_tiny + ((n * k) % n_fft));
+          re = fmaf(xw[n], w.x, re);
+          im = fmaf(xw[n], w.y, im);
+        }
+      }
+      p[k] = apply_power(re * re + im * im, a.power);
+      if (k < nfreq) nonfinite |= !isfinite(p[k]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PST; k++) P_s[tid * PST + k] = p[k];
+    bad_s[tid] = (MODE != MODE_SPECTRUM && nonfinite) ? 1 : 0;
+    __syncthreads();
+    epilogue<MODE, F, THREADS>(a, P_s, PST, nfreq, bad_s, cd, c, t0, mel_s, red_s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// clamp (top_db floor) + DCT-II over the frame-major log-mel
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) dct_kernel(DctArgs a) {
+  constexpr int TT = kDctTile, MC = 128;
+  __shared__ float tile[TT][MC + 1];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  for (int ti = blockIdx.x; ti < a.total_tiles; ti += gridDim.x) {
+    const int c = __ldg(a.tile_clip + ti);
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int tf = __ldg(a.tile_first + ti);
+    const int nt = min(TT, cd.n_frames - tf);
+    const float thr = (a.top_db > 0.0f) ? dec_f(__ldg(a.clip_max + c)) - a.top_db : -INFINITY;
+    const float *src = a.mel_db + (cd.frame_off + tf) * (long long)a.n_mels;
+    const long long T = cd.n_frames;
+    for (int kc = 0; kc < a.n_mfcc; kc += 32) {
+      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      for (int mc = 0; mc < a.n_mels; mc += MC) {
+        const int mw = min(MC, a.n_mels - mc);
+        __syncthreads();
+        for (int i = tid; i < TT * MC; i += 256) {
+          const int r = i / MC, col = i - r * MC;
+          float x = 0.0f;
+          if (r < nt && col < mw) {
+            x = __ldg(src + (long long)r * a.n_mels + mc + col);
+            if (a.top_db > 0.0f) x = vthr(x, thr);
+          }
+          tile[r][col] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int k = kc + w + 8 * q;
+          if (k < a.n_mfcc) {
+            const float *brow = a.basis + (long long)k * a.n_mels + mc;
+            float s = acc[q];
+            for (int n = 0; n < mw; n++) s = fmaf(__ldg(brow + n), tile[lane][n], s);
+            acc[q] = s;
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int k = kc + w + 8 * q;
+        if (k < a.n_mfcc && lane < nt) a.out[cd.out_off + (long long)k * T + tf + lane] = acc[q];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dB scaling over a flat array (mm_power_to_db / mm_amplitude_to_db)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) db_pass1_kernel(const float *x, float *y, long long n,
+                                                       float mult, float amin, float ref,
+                                                       unsigned *slot) {
+  __shared__ float red[8];
+  float vmax = -INFINITY;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const float v = mult * log10f(vthr(x[i], amin) / ref);
+    y[i] = v;
+    vmax = fmaxf(vmax, v);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < 8 ? red[threadIdx.x] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > -INFINITY) atomicMax(slot, enc_f(v));
+  }
+}
+
+__global__ void __launch_bounds__(256) db_pass2_kernel(float *y, long long n, float top_db,
+                                                       const unsigned *slot) {
+  const float thr = dec_f(*slot) - top_db;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
+    y[i] = vthr(y[i], thr);
+}
+
+__global__ void fill_u32_kernel(unsigned *p, unsigned v, long long n) {
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) p[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// table builders: float64 arithmetic on the device, rounded once to float32
+// ---------------------------------------------------------------------------
+__global__ void build_window_kernel(float *w, int n_fft, int win, int zero) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= n_fft) return;
+  double v = 0.0;
+  if (!zero && win > 0) {
+    long long idx;
+    if (win < n_fft) idx = (long long)n - (n_fft - win) / 2;
+    else if (win > n_fft) idx = (long long)n + (win - n_fft) / 2;
+    else idx = n;
+    if (idx >= 0 && idx < win) v = (win == 1) ? 1.0 : 0.5 - 0.5 * cospi(2.0 * (double)idx / (double)win);
+  }
+  w[n] = (float)v;
+}
+
+// exp(-2 pi i t / period) for t = k*r, r in [1,R), k in [0,Ns): stored [r-1][k]
+__global__ void build_stage_tw_kernel(float2 *tw, int R, int Ns) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (R - 1) * Ns) return;
+  const int r = i / Ns + 1, k = i - (r - 1) * Ns;
+  const long long period = (long long)R * Ns;
+  const long long t = ((long long)k * r) % period;
+  double s, c;
+  sincospi(-2.0 * (double)t / (double)period, &s, &c);
+  tw[i] = make_float2((float)c, (float)s);
+}
+
+__global__ void build_roots_kernel(float2 *tw, int count, int period) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  double s, c;
+  sincospi(-2.0 * (double)t / (double)period, &s, &c);
+  tw[t] = make_float2((float)c, (float)s);
+}
+
+__device__ double hz_to_mel_d(double hz) {
+  const double f_sp = 200.0 / 3.0, min_log_mel = 1000.0 / f_sp, logstep = log(6.4) / 27.0;
+  double mel = hz / f_sp;
+  if (hz >= 1000.0) mel = min_log_mel + log(hz / 1000.0) / logstep;
+  return mel;
+}
+__device__ double mel_to_hz_d(double mel) {
+  const double f_sp = 200.0 / 3.0, min_log_mel = 1000.0 / f_sp, logstep = log(6.4) / 27.0;
+  if (mel < min_log_mel) return mel * f_sp;
+  return 1000.0 * exp((mel - min_log_mel) * logstep);
+}
+
+// Dense Slaney filterbank, one thread per (mel, bin) (FilterBank.swift:23-73).
+__global__ void build_mel_kernel(float *W, int sr, int n_fft, int n_mels, double fmin, double fmax) {
+  const int nfreq = n_fft / 2 + 1;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)n_mels * nfreq) return;
+  const int m = (int)(i / nfreq), k = (int)(i - (long long)m * nfreq);
+  const double lo = hz_to_mel_d(fmin), hi = hz_to_mel_d(fmax);
+  const double step = (hi - lo) / (double)(n_mels + 1);
+  const double fl = mel_to_hz_d(lo + m * step);
+  const double fc = mel_to_hz_d(lo + (m + 1) * step);
+  const double fr = mel_to_hz_d(lo + (m + 2) * step);
+  const double f = (double)k * (double)sr / (double)n_fft;
+  double w = 0.0;
+  if (f >= fl && f <= fc && fc != fl) w = (f - fl) / (fc - fl);
+  else if (f > fc && f <= fr && fr != fc) w = (fr - f) / (fr - fc);
+  const double enorm = 2.0 / (fr - fl);
+  W[i] = (float)(w * enorm);
+}
+
+// Per-mel nonzero range of the dense filterbank + NaN-row flag.
+__global__ void build_mel_info_kernel(int4 *info, const float *W, int n_mels, int nfreq) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= n_mels) return;
+  const float *row = W + (long long)m * nfreq;
+  int first = -1, last = -1, nan_row = 0;
+  for (int k = 0; k < nfreq; k++) {
+    const float w = row[k];
+    if (isnan(w)) nan_row = 1;
+    if (w != 0.0f) {
+      if (first < 0) first = k;
+      last = k;
+    }
+  }
+  if (first < 0) info[m] = make_int4(0, 0, m * nfreq, nan_row);
+  else info[m] = make_int4(first, last - first + 1, m * nfreq + first, nan_row);
+}
+
+// DCT-II ortho basis (MFCC.swift:79-88) in float64.
+__global__ void build_dct_kernel(float *B, int n_mfcc, int n_mels) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_mfcc * n_mels) return;
+  const int k = i / n_mels, n = i - k * n_mels;
+  const long long num = ((long long)k * (2LL * n + 1)) % (4LL * n_mels);
+  const double c = cospi((double)num / (2.0 * n_mels));
+  const double s = (k == 0) ? sqrt(1.0 / n_mels) : sqrt(2.0 / n_mels);
+  B[i] = (float)(c * s);
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, float fmin,
+                         float fmax, int n_mfcc_eff, int window_zero, cudaStream_t s) {
+  cudaError_t e;
+  const int nfreq = n_fft / 2 + 1;
+  int log2n = 0;
+  while ((1 << log2n) < n_fft) log2n++;
+  t.n_fft = n_fft;
+  t.n_mels = n_mels;
+  t.n_mfcc = n_mfcc_eff;
+#define MM_TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
+  MM_TRY(cudaMalloc(&t.window, sizeof(float) * (size_t)n_fft));
+  build_window_kernel<<<blocks_for(n_fft, 256), 256, 0, s>>>(t.window, n_fft, win, window_zero);
+  if (log2n >= 5) {
+    const int log2m = log2n - 1;
+    const int cnt = tw_count(log2m);
+    MM_TRY(cudaMalloc(&t.tw_stage, sizeof(float2) * (size_t)(cnt > 0 ? cnt : 1)));
+    const int ns_total = n_stages(log2m);
+    for (int q = 1; q < ns_total; q++) {
+      const int R = stage_radix(log2m, q), Ns = stage_ns(log2m, q);
+      build_stage_tw_kernel<<<blocks_for((long long)(R - 1) * Ns, 256), 256, 0, s>>>(
+          t.tw_stage + stage_tw_off(log2m, q), R, Ns);
+    }
+    const int m4 = n_fft / 4;
+    MM_TRY(cudaMalloc(&t.tw_split, sizeof(float2) * (size_t)m4));
+    build_roots_kernel<<<blocks_for(m4, 256), 256, 0, s>>>(t.tw_split, m4, n_fft);
+  } else {
+    MM_TRY(cudaMalloc(&t.tw_tiny, sizeof(float2) * (size_t)n_fft));
+    build_roots_kernel<<<1, 32, 0, s>>>(t.tw_tiny, n_fft, n_fft);
+  }
+  if (n_mels > 0) {
+    const long long cnt = (long long)n_mels * nfreq;
+    MM_TRY(cudaMalloc(&t.mel_w, sizeof(float) * (size_t)cnt));
+    MM_TRY(cudaMalloc(&t.mel_info, sizeof(int4) * (size_t)n_mels));
+    build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
+                                                          (double)fmax);
+    build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
+  }
+  if (n_mfcc_eff > 0 && n_mels > 0) {
+    MM_TRY(cudaMalloc(&t.dct, sizeof(float) * (size_t)n_mfcc_eff * n_mels));
+    build_dct_kernel<<<blocks_for((long long)n_mfcc_eff * n_mels, 256), 256, 0, s>>>(t.dct, n_mfcc_eff,
+                                                                                      n_mels);
+  }
+#undef MM_TRY
+  return cudaGetLastError();
+}
+
+template <int LOG2N, int F, int MODE>
+static cudaError_t launch_fft_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  using S = Shape<LOG2N>;
+  constexpr int THREADS = S::TPF * F;
+  const size_t smem = fixed_smem_bytes<LOG2N, F>() + (MODE == MODE_SPECTRUM ? 0 : 16 * (size_t)a.n_mels);
+  auto kern = frontend_kernel<LOG2N, F, MODE>;
+  static size_t configured = 0;
+  cudaError_t e;
+  if (smem > 48 * 1024 && smem > configured) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = smem;
+  }
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  long long grid = (long long)sms * per_sm;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  if (grid < 1) return cudaSuccess;
+  kern<<<(unsigned)grid, THREADS, smem, s>>>(a);
+  if (launched) *launched = (int)grid;
+  return cudaGetLastError();
+}
+
+template <int MODE>
+static cudaError_t launch_mode(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  switch (log2n) {
+    case 5: return launch_fft_t<5, 128, MODE>(a, grid_limit, s, launched);
+    case 6: return launch_fft_t<6, 64, MODE>(a, grid_limit, s, launched);
+    case 7: return launch_fft_t<7, 32, MODE>(a, grid_limit, s, launched);
+    case 8: return launch_fft_t<8, 32, MODE>(a, grid_limit, s, launched);
+    case 9: return launch_fft_t<9, 16, MODE>(a, grid_limit, s, launched);
+    case 10: return launch_fft_t<10, 8, MODE>(a, grid_limit, s, launched);
+    case 11: return launch_fft_t<11, 4, MODE>(a, grid_limit, s, launched);
+    case 12: return launch_fft_t<12, 2, MODE>(a, grid_limit, s, launched);
+    case 13: return launch_fft_t<13, 1, MODE>(a, grid_limit, s, launched);
+    case 14: return launch_fft_t<14, 1, MODE>(a, grid_limit, s, launched);
+    case 15: return launch_fft_t<15, 1, MODE>(a, grid_limit, s, launched);
+    default: break;
+  }
+  if (log2n < 0 || log2n > 4) return cudaErrorInvalidValue;
+  const size_t smem = (MODE == MODE_SPECTRUM) ? 0 : 16 * (size_t)a.n_mels;
+  auto kern = frontend_tiny_kernel<MODE>;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long grid = (long long)sms * 4;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  if (grid < 1) return cudaSuccess;
+  kern<<<(unsigned)grid, 128, smem, s>>>(a, 1 << log2n);
+  if (launched) *launched = (int)grid;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_frontend(int log2n, int mode, const FrontArgs &a, int grid_limit, cudaStream_t s,
+                            int *launched) {
+  if (launched) *launched = 0;
+  if (a.total_tiles <= 0) return cudaSuccess;
+  switch (mode) {
+    case MODE_SPECTRUM: return launch_mode<MODE_SPECTRUM>(log2n, a, grid_limit, s, launched);
+    case MODE_MEL: return launch_mode<MODE_MEL>(log2n, a, grid_limit, s, launched);
+    case MODE_MELDB: return launch_mode<MODE_MELDB>(log2n, a, grid_limit, s, launched);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
+  if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long grid = (long long)sms * 8;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  dct_kernel<<<(unsigned)grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_u32(unsigned *p, unsigned v, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  long long g = (n + 255) / 256;
+  if (g > 4096) g = 4096;
+  fill_u32_kernel<<<(unsigned)g, 256, 0, s>>>(p, v, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_db(const float *x, float *y, long long n, float mult, float amin, float ref,
+                      float top_db, unsigned *slot, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  cudaError_t e = launch_fill_u32(slot, encode_max_init(), 1, s);
+  if (e != cudaSuccess) return e;
+  long long g = (n + 255) / 256;
+  if (g > 148 * 16) g = 148 * 16;
+  db_pass1_kernel<<<(unsigned)g, 256, 0, s>>>(x, y, n, mult, amin, ref, slot);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (top_db > 0.0f) {
+    db_pass2_kernel<<<(unsigned)g, 256, 0, s>>>(y, n, top_db, slot);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+}  // namespace mm

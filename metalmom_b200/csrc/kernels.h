@@ -1,0 +1,96 @@
+// Interfaces between the host runtime (mm_runtime.cpp / mm_abi.cpp) and the
+// CUDA kernels (frontend_kernels.cu).  Plain structs and pointers only.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mm {
+
+// One clip of a batch, as the frame kernels see it.
+struct ClipDesc {
+  long long sig_off;    // first sample of the clip in the signal buffer
+  long long length;     // samples in the clip
+  long long frame_off;  // global index of the clip's first frame (frame-major buffers)
+  long long out_off;    // element offset of the clip's [rows x n_frames] output block
+  int n_frames;         // frames of this clip (reference frame count)
+  int tile_base;        // first frame-tile index of this clip
+};
+
+enum FrontMode : int {
+  MODE_SPECTRUM = 0,  // |X|^power per bin -> out[k][t]          (mm_stft)
+  MODE_MEL = 1,       // mel of |X|^power  -> out[m][t]           (mm_mel_spectrogram)
+  MODE_MELDB = 2,     // 10 log10(max(mel,amin)/ref) -> out[frame][m] + per-clip max
+};
+
+enum PadMode : int { PAD_CONSTANT = 0, PAD_REFLECT = 1 };
+
+// Device tables for one (sr, n_fft, win, n_mels, fmin, fmax, n_mfcc) group.
+struct DevTables {
+  int n_fft = 0, n_mels = 0, n_mfcc = 0;
+  float *window = nullptr;   // [n_fft] analysis window (float64-built)
+  float2 *tw_stage = nullptr;  // per-stage Stockham twiddles (layout: stage_twiddle_count)
+  float2 *tw_split = nullptr;  // exp(-2 pi i k / n_fft), k < n_fft/4 (real split)
+  float2 *tw_tiny = nullptr;   // exp(-2 pi i t / n_fft), t < n_fft (n_fft <= 16 only)
+  float *mel_w = nullptr;      // dense [n_mels][n_fft/2+1] float32 weights
+  int4 *mel_info = nullptr;    // per mel {start bin, count, dense offset, nan-row flag}
+  float *dct = nullptr;        // [n_mfcc_eff][n_mels] DCT-II ortho basis
+};
+
+struct FrontArgs {
+  const float *signal;
+  const ClipDesc *clips;
+  const int *tile_clip;  // frame tile -> clip index
+  int total_tiles;
+  int hop, pad, pad_mode;
+  const float *window;
+  const float2 *tw_stage;
+  const float2 *tw_split;
+  const float2 *tw_tiny;
+  const int4 *mel_info;
+  const float *mel_w;
+  int n_mels;
+  float power;  // exponent applied to |X| (2 = power spectrum)
+  float amin, ref;
+  float *out;
+  unsigned *clip_max;  // MODE_MELDB: order-preserving encoded max per clip
+};
+
+struct DctArgs {
+  const float *mel_db;  // [total_frames][n_mels]
+  const ClipDesc *clips;
+  const int *tile_clip;  // DCT tile (kDctTile frames) -> clip
+  const int *tile_first; // first frame (within the clip) of each DCT tile
+  int total_tiles;
+  const unsigned *clip_max;
+  const float *basis;  // [n_mfcc][n_mels]
+  int n_mels, n_mfcc;
+  float top_db;  // <= 0: no floor
+  float *out;    // per clip [n_mfcc][n_frames] at clips[c].out_off
+};
+
+constexpr int kDctTile = 32;
+
+// Frames per CTA tile for a given log2(n_fft).
+int frames_per_tile(int log2n);
+// Stockham twiddle table length (entries) for log2(n_fft) >= 5.
+int stage_twiddle_count(int log2n);
+
+// Table construction (float64 math on the device, stored as float32).
+cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, float fmin,
+                         float fmax, int n_mfcc_eff, int window_zero, cudaStream_t s);
+
+// Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
+cudaError_t launch_frontend(int log2n, int mode, const FrontArgs &a, int grid_limit,
+                            cudaStream_t s, int *launched_grid);
+cudaError_t launch_dct(const DctArgs &a, cudaStream_t s);
+cudaError_t launch_fill_u32(unsigned *p, unsigned v, long long n, cudaStream_t s);
+
+// dB scaling over a flat array: pass 1 writes mult*log10(max(x,amin)/ref) and the
+// encoded max into *slot; pass 2 floors at max - top_db.
+cudaError_t launch_db(const float *x, float *y, long long n, float mult, float amin,
+                      float ref, float top_db, unsigned *slot, cudaStream_t s);
+
+unsigned encode_max_init();  // encoding of -inf
+float decode_max(unsigned u);  // host-side inverse of the max encoding
+
+}  // namespace mm

@@ -1,0 +1,344 @@
+// Host runtime of libmetalmom.so (see runtime.h).
+#include "runtime.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace mm {
+
+int cuda_status(cudaError_t e) {
+  switch (e) {
+    case cudaSuccess: return MM_OK;
+    case cudaErrorMemoryAllocation: return MM_ERR_ALLOC_FAILED;
+    case cudaErrorNoDevice:
+    case cudaErrorInsufficientDriver:
+    case cudaErrorInvalidDevice: return MM_ERR_METAL_UNAVAILABLE;
+    default: return MM_ERR_INTERNAL;
+  }
+}
+
+int gpu_available() {
+  static std::once_flag once;
+  static int status = MM_ERR_METAL_UNAVAILABLE;
+  std::call_once(once, [] {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) == cudaSuccess && n > 0) status = MM_OK;
+    else cudaGetLastError();
+  });
+  return status;
+}
+
+int is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
+int ilog2(long long n) {
+  int l = 0;
+  while ((1LL << l) < n) l++;
+  return l;
+}
+
+long long frame_count(long long length, int n_fft, int hop, int center) {
+  const long long padded = center ? length + 2LL * (n_fft / 2) : length;
+  if (padded < n_fft || !is_pow2(n_fft) || hop <= 0) return 0;
+  return 1 + (padded - n_fft) / hop;
+}
+
+int output_rows(const Group &g) {
+  switch (g.mode) {
+    case MODE_SPECTRUM: return g.n_fft / 2 + 1;
+    case MODE_MEL: return g.n_mels;
+    default: return g.n_mfcc_eff;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// resident tables
+// ---------------------------------------------------------------------------
+namespace {
+struct TableKey {
+  int dev, sr, n_fft, win, window_zero, n_mels, n_mfcc;
+  float fmin, fmax;
+  bool operator<(const TableKey &o) const {
+    return std::tie(dev, sr, n_fft, win, window_zero, n_mels, n_mfcc, fmin, fmax) <
+           std::tie(o.dev, o.sr, o.n_fft, o.win, o.window_zero, o.n_mels, o.n_mfcc, o.fmin, o.fmax);
+  }
+};
+std::mutex g_table_mu;
+std::map<TableKey, DevTables *> g_tables;
+}  // namespace
+
+const DevTables *get_tables(const Group &g, int *status) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    *status = cuda_status(e);
+    return nullptr;
+  }
+  const int n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
+  const int n_mfcc = (g.mode == MODE_MELDB) ? g.n_mfcc_eff : 0;
+  TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax};
+  std::lock_guard<std::mutex> lock(g_table_mu);
+  auto it = g_tables.find(k);
+  if (it != g_tables.end()) {
+    *status = MM_OK;
+    return it->second;
+  }
+  DevTables *t = new DevTables();
+  cudaStream_t s;
+  e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) {
+    e = build_tables(*t, g.sr, g.n_fft, g.win, n_mels, g.fmin, g.fmax, n_mfcc, g.window_zero, s);
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = e2;
+    cudaStreamDestroy(s);
+  }
+  if (e != cudaSuccess) {
+    *status = cuda_status(e);
+    cudaFree(t->window);
+    cudaFree(t->tw_stage);
+    cudaFree(t->tw_split);
+    cudaFree(t->tw_tiny);
+    cudaFree(t->mel_w);
+    cudaFree(t->mel_info);
+    cudaFree(t->dct);
+    delete t;
+    return nullptr;
+  }
+  g_tables[k] = t;
+  *status = MM_OK;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// batch layout
+// ---------------------------------------------------------------------------
+static inline long long round_up(long long v, long long a) { return (v + a - 1) / a * a; }
+
+void make_layout(const Group &g, const int64_t *lengths, int n, Layout &L) {
+  L.clips.resize(n);
+  L.tile_clip.clear();
+  L.dct_tile_clip.clear();
+  L.dct_tile_first.clear();
+  L.F = frames_per_tile(g.log2n);
+  const int rows = output_rows(g);
+  long long sig = 0, frames = 0, out = 0;
+  int tiles = 0;
+  for (int i = 0; i < n; i++) {
+    ClipDesc &c = L.clips[i];
+    const long long T = frame_count(lengths[i], g.n_fft, g.hop, g.center);
+    c.sig_off = sig;
+    c.length = lengths[i];
+    c.frame_off = frames;
+    c.out_off = out;
+    c.n_frames = (int)T;
+    c.tile_base = tiles;
+    const int nt = (int)((T + L.F - 1) / L.F);
+    for (int q = 0; q < nt; q++) L.tile_clip.push_back(i);
+    tiles += nt;
+    if (g.mode == MODE_MELDB)
+      for (long long f = 0; f < T; f += kDctTile) {
+        L.dct_tile_clip.push_back(i);
+        L.dct_tile_first.push_back((int)f);
+      }
+    sig = round_up(sig + lengths[i], 4);
+    frames += T;
+    out += (long long)rows * T;
+  }
+  L.sig_elems = sig;
+  L.total_frames = frames;
+  L.out_elems = out;
+  L.meldb_elems = (g.mode == MODE_MELDB) ? frames * (long long)g.n_mels : 0;
+}
+
+namespace {
+struct Offsets {
+  size_t signal, clips, tile_clip, dct_clip, dct_first, desc_end, clip_max, meldb, out, total;
+};
+Offsets offsets(const Layout &L) {
+  Offsets o;
+  const size_t n = L.clips.size();
+  size_t p = 0;
+  o.signal = p;
+  p = round_up(p + sizeof(float) * (size_t)L.sig_elems, 256);
+  o.clips = p;
+  p = round_up(p + sizeof(ClipDesc) * n, 16);
+  o.tile_clip = p;
+  p = round_up(p + sizeof(int) * L.tile_clip.size(), 16);
+  o.dct_clip = p;
+  p = round_up(p + sizeof(int) * L.dct_tile_clip.size(), 16);
+  o.dct_first = p;
+  p = round_up(p + sizeof(int) * L.dct_tile_first.size(), 16);
+  o.desc_end = p;
+  p = round_up(p, 256);
+  o.clip_max = p;
+  p = round_up(p + sizeof(unsigned) * (n > 0 ? n : 1), 256);
+  o.meldb = p;
+  p = round_up(p + sizeof(float) * (size_t)L.meldb_elems, 256);
+  o.out = p;
+  p = round_up(p + sizeof(float) * (size_t)L.out_elems, 256);
+  o.total = p;
+  return o;
+}
+}  // namespace
+
+size_t arena_bytes(const Group &, const Layout &L) { return offsets(L).total; }
+
+size_t carve_arena(const Group &, const Layout &L, char *base, DevBatch &b) {
+  const Offsets o = offsets(L);
+  b.signal = reinterpret_cast<float *>(base + o.signal);
+  b.clips = reinterpret_cast<ClipDesc *>(base + o.clips);
+  b.tile_clip = reinterpret_cast<int *>(base + o.tile_clip);
+  b.dct_tile_clip = reinterpret_cast<int *>(base + o.dct_clip);
+  b.dct_tile_first = reinterpret_cast<int *>(base + o.dct_first);
+  b.clip_max = reinterpret_cast<unsigned *>(base + o.clip_max);
+  b.meldb = reinterpret_cast<float *>(base + o.meldb);
+  b.out = reinterpret_cast<float *>(base + o.out);
+  return o.desc_end - o.clips;
+}
+
+void pack_descriptors(const Layout &L, char *host) {
+  // host mirrors the arena from the clips segment on
+  const Offsets o = offsets(L);
+  if (!L.clips.empty()) memcpy(host, L.clips.data(), sizeof(ClipDesc) * L.clips.size());
+  if (!L.tile_clip.empty())
+    memcpy(host + (o.tile_clip - o.clips), L.tile_clip.data(), sizeof(int) * L.tile_clip.size());
+  if (!L.dct_tile_clip.empty())
+    memcpy(host + (o.dct_clip - o.clips), L.dct_tile_clip.data(), sizeof(int) * L.dct_tile_clip.size());
+  if (!L.dct_tile_first.empty())
+    memcpy(host + (o.dct_first - o.clips), L.dct_tile_first.data(), sizeof(int) * L.dct_tile_first.size());
+}
+
+cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, const DevBatch &b,
+                          cudaStream_t s, cudaEvent_t *ev, int *n_launches) {
+  cudaError_t e;
+  int launches = 0;
+  if (ev && (e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+  const int n = (int)L.clips.size();
+  if (g.mode == MODE_MELDB) {
+    if ((e = launch_fill_u32(b.clip_max, encode_max_init(), n, s)) != cudaSuccess) return e;
+    launches++;
+  }
+  if (ev && (e = cudaEventRecord(ev[1], s)) != cudaSuccess) return e;
+  FrontArgs a;
+  a.signal = b.signal;
+  a.clips = b.clips;
+  a.tile_clip = b.tile_clip;
+  a.total_tiles = (int)L.tile_clip.size();
+  a.hop = g.hop;
+  a.pad = g.center ? g.n_fft / 2 : 0;
+  a.pad_mode = g.pad_mode;
+  a.window = t->window;
+  a.tw_stage = t->tw_stage;
+  a.tw_split = t->tw_split;
+  a.tw_tiny = t->tw_tiny;
+  a.mel_info = t->mel_info;
+  a.mel_w = t->mel_w;
+  a.n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
+  a.power = g.power;
+  a.amin = g.amin;
+  a.ref = g.ref;
+  a.out = (g.mode == MODE_MELDB) ? b.meldb : b.out;
+  a.clip_max = b.clip_max;
+  int grid = 0;
+  if ((e = launch_frontend(g.log2n, g.mode, a, 0, s, &grid)) != cudaSuccess) return e;
+  if (grid > 0) launches++;
+  if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
+  if (g.mode == MODE_MELDB && g.n_mfcc_eff > 0 && !L.dct_tile_clip.empty()) {
+    DctArgs d;
+    d.mel_db = b.meldb;
+    d.clips = b.clips;
+    d.tile_clip = b.dct_tile_clip;
+    d.tile_first = b.dct_tile_first;
+    d.total_tiles = (int)L.dct_tile_clip.size();
+    d.clip_max = b.clip_max;
+    d.basis = t->dct;
+    d.n_mels = g.n_mels;
+    d.n_mfcc = g.n_mfcc_eff;
+    d.top_db = g.top_db;
+    d.out = b.out;
+    if ((e = launch_dct(d, s)) != cudaSuccess) return e;
+    launches++;
+  }
+  if (ev && (e = cudaEventRecord(ev[3], s)) != cudaSuccess) return e;
+  if (n_launches) *n_launches = launches;
+  return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// per-thread workspace
+// ---------------------------------------------------------------------------
+namespace {
+struct WorkspaceHolder {
+  Workspace ws;
+  ~WorkspaceHolder() {
+    // Process teardown may already have destroyed the CUDA context; ignore errors.
+    if (ws.stream) cudaStreamDestroy(ws.stream);
+    if (ws.dev) cudaFree(ws.dev);
+    if (ws.host) cudaFreeHost(ws.host);
+  }
+};
+thread_local WorkspaceHolder t_ws;
+}  // namespace
+
+int thread_workspace(size_t dev_bytes, size_t host_bytes, Workspace **out) {
+  Workspace &w = t_ws.ws;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (w.device != dev) {
+    // First use on this thread, or the caller switched devices: start over.
+    if (w.stream) {
+      cudaStreamSynchronize(w.stream);
+      cudaStreamDestroy(w.stream);
+      w.stream = nullptr;
+    }
+    if (w.dev) cudaFree(w.dev);  // unified addressing: frees on its own device
+    w.dev = nullptr;
+    w.dev_bytes = 0;
+    e = cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_status(e);
+    w.device = dev;
+  }
+  if (dev_bytes > w.dev_bytes) {
+    cudaStreamSynchronize(w.stream);
+    if (w.dev) cudaFree(w.dev);
+    w.dev = nullptr;
+    w.dev_bytes = 0;
+    const size_t want = dev_bytes + dev_bytes / 4;
+    e = cudaMalloc(&w.dev, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return MM_ERR_ALLOC_FAILED;
+    }
+    w.dev_bytes = want;
+  }
+  if (host_bytes > w.host_bytes) {
+    cudaStreamSynchronize(w.stream);
+    if (w.host) cudaFreeHost(w.host);
+    w.host = nullptr;
+    w.host_bytes = 0;
+    const size_t want = host_bytes + host_bytes / 4;
+    e = cudaMallocHost(&w.host, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return MM_ERR_ALLOC_FAILED;
+    }
+    w.host_bytes = want;
+  }
+  *out = &w;
+  return MM_OK;
+}
+
+void fill_buffer(MMBuffer *out, float *data, long long rows, long long cols) {
+  out->data = data;
+  for (int i = 0; i < 8; i++) out->shape[i] = 0;
+  out->shape[0] = rows;
+  out->shape[1] = cols;
+  out->ndim = 2;
+  out->dtype = 0;
+  out->count = rows * cols;
+}
+
+}  // namespace mm

@@ -1,0 +1,271 @@
+"""GPU parity: the CUDA path through the C ABI against the FP64 oracle and the
+reference's golden vectors.
+
+Tolerances (stated per test):
+  * golden vectors -- the reference's own (rtol=atol=1e-4; 5e-4 for the
+    fmin=300/fmax=8000 MFCC), Tests/test_parity_*.py;
+  * mel-dB vs FP64 oracle -- 1e-3 dB max abs after the top_db floor;
+  * MFCC vs FP64 oracle -- 1e-4 of max |c| per clip;
+  * linear spectra vs FP64 oracle -- 2e-5 of the frame-set maximum (float32 FFT);
+  * frame counts, padding and shapes -- exact.
+"""
+
+import numpy as np
+import pytest
+
+import metalmom_b200 as M
+from metalmom_b200 import synth
+from goldens import golden, signal_440
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SR = 22050
+DB_TOL = 1e-3
+MFCC_TOL = 1e-4
+
+
+def _db_from_power(P, top_db=80.0):
+    return O.power_to_db(np.asarray(P, np.float64), 1.0, 1e-10, top_db)
+
+
+# ---------------------------------------------------------------------------
+# golden vectors (the reference's tests, run against the CUDA path)
+# ---------------------------------------------------------------------------
+
+def test_stft_golden():
+    y = signal_440()
+    exp = golden("stft_440hz_default_magnitude")
+    got = M.stft(y, n_fft=2048, hop_length=512, win_length=2048, center=True)
+    assert got.shape == exp.shape and got.dtype == np.float32
+    np.testing.assert_allclose(got, exp, rtol=1e-4, atol=1e-4)
+    mid = got.shape[1] // 2
+    assert np.argmax(got[:, mid]) == np.argmax(exp[:, mid])
+    assert 0.99 < np.sum(got.astype(np.float64) ** 2) / np.sum(exp.astype(np.float64) ** 2) < 1.01
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("mel_spectrogram_440hz_default", dict()),
+    ("mel_spectrogram_440hz_40_1024", dict(n_fft=1024, n_mels=40)),
+    ("mel_spectrogram_440hz_64_fmin300_fmax8000", dict(n_fft=2048, n_mels=64, fmin=300, fmax=8000)),
+])
+def test_melspectrogram_golden(name, kw):
+    exp = golden(name)
+    got = M.melspectrogram(y=signal_440(), sr=SR, **kw)
+    assert got.shape == exp.shape and got.dtype == np.float32
+    np.testing.assert_allclose(got, exp, rtol=1e-4, atol=1e-4)
+    assert np.all(got >= 0)
+
+
+@pytest.mark.parametrize("name,kw,tol", [
+    ("mfcc_440hz_default", dict(), 1e-4),
+    ("mfcc_440hz_13_1024", dict(n_mfcc=13, n_fft=1024, n_mels=40), 1e-4),
+    ("mfcc_440hz_20_64_fmin300_fmax8000", dict(n_mfcc=20, n_fft=2048, n_mels=64, fmin=300, fmax=8000), 5e-4),
+])
+def test_mfcc_golden(name, kw, tol):
+    exp = golden(name)
+    got = M.mfcc(y=signal_440(), sr=SR, **kw)
+    assert got.shape == exp.shape and got.dtype == np.float32
+    np.testing.assert_allclose(got, exp, rtol=tol, atol=tol)
+    assert np.all(np.isfinite(got))
+
+
+def test_db_goldens():
+    S = golden("stft_440hz_default_magnitude").astype(np.float32)
+    np.testing.assert_allclose(M.amplitude_to_db(S, ref=np.max), golden("stft_440hz_amplitude_db"),
+                               rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(M.amplitude_to_db(S, ref=1.0), golden("stft_440hz_amplitude_db_ref1"),
+                               rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(M.power_to_db(S ** 2, ref=np.max), golden("stft_440hz_power_db"),
+                               rtol=1e-4, atol=1e-4)
+
+
+# ---------------------------------------------------------------------------
+# FP64 oracle, across every supported FFT size and the padding/window cases
+# ---------------------------------------------------------------------------
+
+ALL_NFFT = [2 ** k for k in range(0, 16)]
+
+
+@pytest.mark.parametrize("n_fft", ALL_NFFT)
+def test_stft_all_sizes_vs_oracle(n_fft):
+    rng = np.random.default_rng(n_fft)
+    L = max(3 * n_fft + 17, 64)
+    y = rng.standard_normal(L).astype(np.float32)
+    hop = max(1, n_fft // 4)
+    got = M.stft(y, n_fft=n_fft, hop_length=hop)
+    exp = O.stft_magnitude(y, n_fft, hop, n_fft, True)
+    assert got.shape == exp.shape == (n_fft // 2 + 1, O.n_frames(L, n_fft, hop, True))
+    err = np.abs(got - exp).max() / exp.max()
+    assert err < 2e-5, err
+
+
+@pytest.mark.parametrize("n_fft,hop,win,center,L", [
+    (2048, 512, 2048, True, 661500 // 10),
+    (2048, 512, 2048, False, 50000),
+    (512, 160, 400, True, 16000),      # window shorter than n_fft (centred, zero-padded)
+    (2048, 512, 4096, True, 22050),    # window longer than n_fft (centre-truncated)
+    (1024, 4096, 1024, True, 22050),   # hop longer than n_fft
+    (2048, 441, 2048, True, 30001),    # odd hop: unaligned frame starts
+    (1024, 256, 1024, True, 1),        # single sample, centred -> 1 frame
+    (1024, 256, 1024, True, 300),      # shorter than n_fft/2
+    (4096, 1024, 4096, True, 123457),
+    (256, 64, 200, False, 9999),
+])
+def test_stft_cases_vs_oracle(n_fft, hop, win, center, L):
+    y = synth.music_clip(L, SR, seed=L + n_fft)
+    got = M.stft(y, n_fft=n_fft, hop_length=hop, win_length=win, center=center)
+    exp = O.stft_magnitude(y, n_fft, hop, win, center)
+    assert got.shape == exp.shape
+    if exp.size:
+        assert np.abs(got - exp).max() <= 2e-5 * max(exp.max(), 1e-30)
+
+
+@pytest.mark.parametrize("power", [2.0, 1.0, 1.5])
+def test_mel_power_variants_vs_oracle(power):
+    y = synth.music_clip(44100, SR, seed=7)
+    got = M.melspectrogram(y, sr=SR, n_fft=2048, hop_length=512, power=power)
+    exp = O.melspectrogram(y, SR, 2048, 512, 2048, True, power, 128)
+    assert got.shape == exp.shape
+    assert np.abs(got - exp).max() <= 1e-5 * exp.max()
+    if power == 2.0:
+        mx, _ = O.mel_db_error(_db_from_power(got), _db_from_power(exp))
+        assert mx < DB_TOL, mx
+
+
+@pytest.mark.parametrize("sr,n_fft,hop,win,n_mels,n_mfcc,fmin,fmax,L", [
+    (22050, 2048, 512, 2048, 128, 20, 0.0, None, 661500),   # the 30 s workload clip
+    (16000, 512, 160, 400, 80, 13, 20.0, 8000.0, 160000),   # speech front end
+    (44100, 4096, 1024, 4096, 64, 20, 0.0, None, 441000),
+    (22050, 1024, 256, 1024, 40, 40, 0.0, None, 22050),     # n_mfcc == n_mels
+    (22050, 2048, 512, 2048, 40, 200, 0.0, None, 22050),    # n_mfcc > n_mels -> capped
+    (22050, 256, 64, 256, 32, 1, 0.0, None, 5000),          # single coefficient
+])
+def test_mfcc_and_meldb_vs_oracle(sr, n_fft, hop, win, n_mels, n_mfcc, fmin, fmax, L):
+    y = (synth.speech_clip if sr == 16000 else synth.music_clip)(L, sr, seed=L ^ n_fft)
+    got = M.mfcc(y, sr=sr, n_mfcc=n_mfcc, n_fft=n_fft, hop_length=hop, win_length=win,
+                 n_mels=n_mels, fmin=fmin, fmax=fmax)
+    exp = O.mfcc(y, sr, n_mfcc, n_fft, hop, win, n_mels, fmin, fmax, True)
+    assert got.shape == exp.shape == (min(n_mfcc, n_mels), O.n_frames(L, n_fft, hop, True))
+    assert O.mfcc_rel_error(got, exp) < MFCC_TOL
+    mel = M.melspectrogram(y, sr=sr, n_fft=n_fft, hop_length=hop, win_length=win, n_mels=n_mels,
+                           fmin=fmin, fmax=fmax)
+    mx, _ = O.mel_db_error(_db_from_power(mel),
+                           O.mel_db(y, sr, n_fft, hop, win, True, n_mels, fmin, fmax))
+    assert mx < DB_TOL, mx
+
+
+def test_power_to_db_vs_oracle():
+    rng = np.random.default_rng(3)
+    S = (rng.random((300, 77)) ** 6).astype(np.float32)
+    for top_db in (80.0, 30.0, None):
+        got = M.power_to_db(S, ref=1.0, top_db=top_db)
+        exp = O.power_to_db(S.astype(np.float64), 1.0, 1e-10, top_db)
+        assert np.abs(got - exp).max() < 1e-4
+    got = M.amplitude_to_db(S, ref=np.max, top_db=60.0)
+    assert got.min() >= got.max() - 60.0 - 1e-4
+
+
+# ---------------------------------------------------------------------------
+# edge cases the reference tests (EdgeCaseTests.swift, test_bridge_errors.py)
+# ---------------------------------------------------------------------------
+
+def test_silence_and_constant():
+    z = np.zeros(22050, np.float32)
+    assert np.all(M.stft(z) == 0.0)
+    assert np.max(M.melspectrogram(z)) < 1e-10
+    c = M.mfcc(z)
+    assert np.all(np.isfinite(c))
+    np.testing.assert_allclose(c, O.mfcc(z, SR, 20, 2048, 512, 2048, 128), atol=1e-3)
+    one = np.ones(22050, np.float32)
+    S = M.stft(one)
+    mid = S.shape[1] // 2
+    assert S[0, mid] > S[1:, mid].mean()
+
+
+def test_nan_and_inf_inputs_do_not_crash():
+    y = np.zeros(4096, np.float32)
+    y[100] = np.nan
+    y[500] = np.nan
+    S = M.stft(y)
+    assert S.shape == (1025, 9)
+    y2 = np.zeros(4096, np.float32)
+    y2[200] = np.inf
+    y2[300] = -np.inf
+    assert M.stft(y2).shape == (1025, 9)
+    m = M.melspectrogram(y)
+    assert m.shape == (128, 9)
+    c = M.mfcc(y)
+    assert c.shape == (20, 9)
+    big = np.full(4096, np.finfo(np.float32).max / 1000, np.float32)
+    assert M.stft(big).shape == (1025, 9)
+
+
+def test_int_input_and_short_signal():
+    assert M.stft(np.ones(2048, dtype=np.int32)).dtype == np.float32
+    y = np.sin(np.arange(10, dtype=np.float32))
+    S = M.stft(y)
+    assert S.shape == (1025, 1)
+    np.testing.assert_allclose(S, O.stft_magnitude(y, 2048, 512, 2048, True), atol=1e-5)
+
+
+def test_buffer_freed_when_reshape_fails():
+    from metalmom_b200._native import ffi, lib
+    from metalmom_b200._buffer import buffer_to_numpy
+    ctx = lib.mm_init()
+    try:
+        y = np.sin(np.arange(4096, dtype=np.float32))
+        p = ffi.new("MMSTFTParams*")
+        p.n_fft, p.hop_length, p.win_length, p.center = 2048, 512, 2048, 1
+        out = ffi.new("MMBuffer*")
+        assert lib.mm_stft(ctx, ffi.cast("const float*", y.ctypes.data), len(y), 22050, p, out) == 0
+        assert out.count > 0
+        out.shape[0] = 9999
+        out.shape[1] = 9999
+        with pytest.raises(ValueError):
+            buffer_to_numpy(out)
+        assert out.data == ffi.NULL
+    finally:
+        lib.mm_destroy(ctx)
+
+
+# ---------------------------------------------------------------------------
+# batching: uneven clips in one launch == per-clip calls; plans + graphs
+# ---------------------------------------------------------------------------
+
+def test_mfcc_batch_matches_single_clip_calls():
+    rng = np.random.default_rng(11)
+    lens = [int(x) for x in rng.integers(1, 90000, 9)] + [1, 1023, 1024, 1025]
+    clips = [synth.music_clip(L, SR, seed=i) for i, L in enumerate(lens)]
+    outs = M.mfcc_batch(clips, sr=SR, n_fft=2048, hop_length=512)
+    for c, o in zip(clips, outs):
+        single = M.mfcc(c, sr=SR, n_fft=2048, hop_length=512)
+        assert o.shape == single.shape
+        np.testing.assert_array_equal(o, single)
+        exp = O.mfcc(c, SR, 20, 2048, 512, 2048, 128)
+        assert O.mfcc_rel_error(o, exp) < MFCC_TOL
+
+
+def test_reflect_padding_vs_oracle():
+    clips = [synth.music_clip(L, SR, seed=L) for L in (5000, 22050, 1500)]
+    outs = M.mfcc_batch(clips, sr=SR, n_fft=2048, hop_length=512, pad_mode="reflect")
+    for c, o in zip(clips, outs):
+        exp = O.mfcc(c, SR, 20, 2048, 512, 2048, 128, pad_mode=O.PAD_REFLECT)
+        assert O.mfcc_rel_error(o, exp) < MFCC_TOL
+    const = M.mfcc_batch(clips[:1], sr=SR, n_fft=2048, hop_length=512)[0]
+    assert np.abs(const - outs[0]).max() > 1e-2  # the two paddings really differ
+
+
+def test_plan_graph_replay_and_host_io():
+    rng = np.random.default_rng(5)
+    lens = [int(x) for x in rng.integers(20000, 120000, 6)]
+    clips = [synth.music_clip(L, SR, seed=100 + i) for i, L in enumerate(lens)]
+    ref = M.mfcc_batch(clips, sr=SR)
+    with M.Plan(lens, sr=SR) as plan:
+        assert plan.frames == [r.shape[1] for r in ref]
+        assert plan.kernel_launches == 3
+        a = plan.execute_host(clips)
+        b = plan.execute_host(clips)
+        for x, y_, r in zip(a, b, ref):
+            np.testing.assert_array_equal(x, y_)
+            np.testing.assert_array_equal(x, r)

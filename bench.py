@@ -176,8 +176,12 @@ def run_ours(args, rank, world, local_rank):
     clips = make_clips(n_clips, seed0=1000 * rank)
     lengths = [len(c) for c in clips]
     plan = M.Plan(lengths, sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
-    stream = torch.cuda.current_stream()
+    # an explicit stream: handle 0 (the legacy default stream) would mean "the
+    # plan's own stream" to the C ABI, outside these events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
+    assert sh != 0
 
     # pinned host buffers for the end-to-end leg
     pin_in = [torch.from_numpy(c).pin_memory() for c in clips]
@@ -324,8 +328,8 @@ def run_reference(args, rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--clips", type=int, default=N_CLIPS)
     ap.add_argument("--e2e-steps", type=int, default=5)

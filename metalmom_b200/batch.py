@@ -46,7 +46,7 @@ def mfcc_batch(clips, **params):
         status = lib.mm_mfcc_batch(ctx, ptrs, lens, n, p, outs)
         if status != 0:
             raise RuntimeError(f"mm_mfcc_batch failed with status {status}")
-        return [buffer_to_numpy(outs[i]) for i in range(n)]
+        return [buffer_to_numpy(outs + i) for i in range(n)]
     finally:
         lib.mm_destroy(ctx)
 

@@ -175,6 +175,8 @@ def run_ours(args, rank, world, local_rank):
     n_clips = args.clips
     clips = make_clips(n_clips, seed0=1000 * rank)
     lengths = [len(c) for c in clips]
+    tune = M.autotune(clip_samples=CLIP_SAMPLES, n_clips=min(n_clips, 64), reps=5, sr=SR,
+                      n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
     plan = M.Plan(lengths, sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
     # an explicit stream: handle 0 (the legacy default stream) would mean "the
     # plan's own stream" to the C ABI, outside these events
@@ -283,6 +285,8 @@ def run_ours(args, rank, world, local_rank):
                     "api": "Plan.execute_host (mm_plan_execute_host)"},
             "clocks": clk.summary(),
             "gpu_launches": K * plan.kernel_launches,
+            "autotune": {"variant": tune["best"], "variant_ms": tune["ms"],
+                         "sample": f"{min(n_clips, 64)} clips of the workload shape"},
         }
         if not args.no_cpu:
             result.update(baseline_leg(plan, clips, world, args))

@@ -164,6 +164,17 @@ MM_API int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float* ms3);
 MM_API int32_t mm_plan_execute_host(mm_plan plan, const float* const* signals, float* const* outs,
                              void* stream);
 
+/* Autotuning of the frame kernel's launch variant (frames per CTA and
+ * register budget), process-wide per n_fft.  mm_autotune times every variant
+ * on n_clips synthetic clips of clip_samples samples (reps launches each),
+ * writes the per-variant milliseconds to variant_ms (up to 3 entries), keeps
+ * the fastest and returns it in *best_variant.  Plans and calls made
+ * afterwards use the tuned variant. */
+MM_API int32_t mm_autotune(mm_context ctx, const MMFrontEndParams* params, int64_t clip_samples,
+                           int32_t n_clips, int32_t reps, float* variant_ms, int32_t* best_variant);
+MM_API int32_t mm_tune_set(int32_t n_fft, int32_t variant);
+MM_API int32_t mm_tune_get(int32_t n_fft);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,7 @@ batched, device-resident path.
 
 from .core import stft
 from .feature import amplitude_to_db, melspectrogram, mfcc, power_to_db
-from .batch import Plan, frontend_params, mfcc_batch
+from .batch import Plan, autotune, frontend_params, mfcc_batch, tune_get, tune_set
 
 __all__ = ["stft", "melspectrogram", "mfcc", "power_to_db", "amplitude_to_db",
-           "mfcc_batch", "Plan", "frontend_params"]
+           "mfcc_batch", "Plan", "frontend_params", "autotune", "tune_get", "tune_set"]

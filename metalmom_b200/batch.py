@@ -31,6 +31,34 @@ def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, cent
     return p
 
 
+def autotune(clip_samples=661500, n_clips=32, reps=10, **params):
+    """Time every launch variant of the frame kernel for these parameters on
+    synthetic clips, keep the fastest for this n_fft (process-wide) and return
+    {"best": v, "ms": [per-variant ms]}."""
+    p = frontend_params(**params)
+    ms = ffi.new("float[3]")
+    best = ffi.new("int32_t*")
+    ctx = lib.mm_init()
+    try:
+        st = lib.mm_autotune(ctx, p, clip_samples, n_clips, reps, ms, best)
+        if st != 0:
+            raise RuntimeError(f"mm_autotune failed with status {st}")
+    finally:
+        lib.mm_destroy(ctx)
+    n = 3 if ms[1] > 0 else 1
+    return {"best": int(best[0]), "ms": [float(ms[i]) for i in range(n)]}
+
+
+def tune_set(n_fft, variant):
+    st = lib.mm_tune_set(n_fft, variant)
+    if st != 0:
+        raise RuntimeError(f"mm_tune_set failed with status {st}")
+
+
+def tune_get(n_fft):
+    return int(lib.mm_tune_get(n_fft))
+
+
 def mfcc_batch(clips, **params):
     """MFCC of every clip in one batched launch sequence; returns a list of arrays."""
     clips = [np.ascontiguousarray(c, dtype=np.float32) for c in clips]

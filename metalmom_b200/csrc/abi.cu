@@ -26,9 +26,11 @@ std::unordered_set<void *> g_ctx;
 
 // Run one clip (n = 1) or a batch of clips through `g`; on success *outs[i]
 // holds a malloc'd [rows x n_frames_i] block (NULL when empty).
-int run_batch(const Group &g, const float *const *signals, const int64_t *lengths, int n,
+int run_batch(const Group &g_in, const float *const *signals, const int64_t *lengths, int n,
               float **outs) {
   for (int i = 0; i < n; i++) outs[i] = nullptr;
+  Group g = g_in;
+  g.variant = group_variant(g);
   Layout L;
   make_layout(g, lengths, n, L);
   if (L.total_frames == 0 || L.out_elems == 0) return MM_OK;
@@ -340,6 +342,7 @@ mm_plan mm_plan_create(mm_context ctx, const MMFrontEndParams *params, const int
     return nullptr;
   }
   cudaGetDevice(&p->device);
+  p->g.variant = group_variant(p->g);
   make_layout(p->g, lengths, n_clips, p->L);
   cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&p->arena, arena_bytes(p->g, p->L));
@@ -450,6 +453,73 @@ int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *c
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return cuda_status(e);
+}
+
+int32_t mm_tune_set(int32_t n_fft, int32_t variant) {
+  if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 || variant > 2) return MM_ERR_INVALID_INPUT;
+  set_tuned_variant(ilog2(n_fft), variant);
+  return MM_OK;
+}
+
+int32_t mm_tune_get(int32_t n_fft) {
+  if (!is_pow2(n_fft) || ilog2(n_fft) > 15) return MM_ERR_INVALID_INPUT;
+  return tuned_variant(ilog2(n_fft));
+}
+
+int32_t mm_autotune(mm_context ctx, const MMFrontEndParams *params, int64_t clip_samples,
+                    int32_t n_clips, int32_t reps, float *variant_ms, int32_t *best_variant) {
+  if (!ctx || clip_samples <= 0 || n_clips <= 0 || reps <= 0) return MM_ERR_INVALID_INPUT;
+  Group g;
+  int st = resolve_frontend(params, g);
+  if (st != MM_OK) return st;
+  if ((st = gpu_available()) != MM_OK) return st;
+  const DevTables *t = get_tables(g, &st);
+  if (!t) return st;
+  const int nv = frame_variants(g.log2n, g.mode, 1);
+  std::vector<int64_t> lengths(n_clips, clip_samples);
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  float best_ms = 0.0f;
+  int best = 0;
+  for (int v = 0; v < nv && e == cudaSuccess; v++) {
+    Group gv = g;
+    gv.variant = v;
+    Layout L;
+    make_layout(gv, lengths.data(), n_clips, L);
+    char *arena = nullptr;
+    e = cudaMalloc(&arena, arena_bytes(gv, L));
+    if (e != cudaSuccess) break;
+    DevBatch b;
+    const size_t desc = carve_arena(gv, L, arena, b);
+    std::vector<char> host(desc + 16);
+    pack_descriptors(L, host.data());
+    e = cudaMemcpyAsync(b.clips, host.data(), desc, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = launch_fill_pattern(b.signal, L.sig_elems, s);
+    for (int w = 0; w < 2 && e == cudaSuccess; w++) e = enqueue_batch(gv, L, t, b, s, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = enqueue_batch(gv, L, t, b, s, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaFree(arena);
+    ms /= reps;
+    if (variant_ms) variant_ms[v] = ms;
+    if (e == cudaSuccess && (v == 0 || ms < best_ms)) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (s) cudaStreamDestroy(s);
+  if (e != cudaSuccess) return cuda_status(e);
+  set_tuned_variant(g.log2n, best);
+  if (best_variant) *best_variant = best;
+  return MM_OK;
 }
 
 }  // extern "C"

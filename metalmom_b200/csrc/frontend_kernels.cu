@@ -1,11 +1,14 @@
 // Frame kernels for the spectral front end on sm_100a.
 //
-// One CTA tile = F consecutive frames of one clip.  Per frame:
+// One CTA tile = F consecutive frames of one clip; each frame is owned by a
+// group of TPF = n_fft/32 threads that synchronise on their own named barrier.
+// Per frame:
 //   gather + window (float2 loads straight from HBM, padding handled in the
 //   index math) -> complex FFT of n_fft/2 points (Stockham, radix-16 stages in
 //   registers, exchanges through bank-padded shared memory) -> real split ->
 //   |X|^2 -> mode epilogue (spectrum rows, mel rows, or log-mel + per-clip max).
-// A second kernel applies the clip-global top_db floor and the DCT-II.
+// A second kernel applies the clip-global top_db floor and the DCT-II as a
+// register-blocked tile product.
 //
 // Reference semantics followed (MetalMom, Sources/MetalMomCore):
 //   frame count / zero padding   Spectral/STFT.swift:241-254
@@ -16,6 +19,8 @@
 //   DCT-II ortho                 Features/MFCC.swift:65-106
 #include <math.h>
 #include <string.h>
+
+#include <algorithm>
 
 #include "fft_radix.cuh"
 #include "kernels.h"
@@ -51,11 +56,12 @@ float decode_max(unsigned u) {
 // vDSP_vthr: x if x >= t else t (a NaN x becomes t).
 __device__ __forceinline__ float vthr(float x, float t) { return x >= t ? x : t; }
 
+// |X|^power from |X|^2: PW 0 -> |X|^2, 1 -> |X|, 2 -> |X|^power.
+template <int PW>
 __device__ __forceinline__ float apply_power(float pw, float power) {
-  if (power == 2.0f) return pw;
-  float mag = sqrtf(pw);
-  if (power == 1.0f) return mag;
-  return powf(mag, power);
+  if constexpr (PW == 0) return pw;
+  else if constexpr (PW == 1) return sqrtf(pw);
+  else return powf(sqrtf(pw), power);
 }
 
 __device__ __forceinline__ long long reflect_idx(long long i, long long L) {
@@ -90,6 +96,40 @@ __device__ __forceinline__ cpx ldc(const float2 *p) {
   return {v.x, v.y};
 }
 
+// Barrier over the TPF threads of frame group f, returning the OR of `pred`
+// over the group.  Groups of >= 32 threads use named barrier f+1; smaller
+// groups live inside one warp.
+template <int TPF>
+__device__ __forceinline__ bool frame_sync_or(int f, bool pred) {
+  if constexpr (TPF >= 32) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((unsigned)pred), "r"(f + 1), "r"(TPF)
+        : "memory");
+    return r != 0;
+  } else {
+    __syncwarp();
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned mask = ((TPF == 32) ? 0xffffffffu : ((1u << TPF) - 1u)) << (lane & ~(unsigned)(TPF - 1));
+    const unsigned b = __ballot_sync(0xffffffffu, pred);
+    return (b & mask) != 0;
+  }
+}
+
+template <int TPF>
+__device__ __forceinline__ void frame_sync(int f) {
+  if constexpr (TPF >= 32) {
+    asm volatile("bar.sync %0, %1;" ::"r"(f + 1), "r"(TPF) : "memory");
+  } else {
+    __syncwarp();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // FFT shape for a real frame of N = 2^LOG2N samples (complex length M = N/2):
 // radix-16 stages followed by one radix-RLAST stage when log2(M) % 4 != 0.
@@ -119,30 +159,76 @@ struct Shape {
   static constexpr int RLAST = 1 << (LOG2M % 4);
   static constexpr int PADM = M + M / 16;
   static constexpr int FSTRIDE = PADM + 1;  // complex slots per frame (odd: spreads banks)
-  static constexpr bool TW_SMEM = (M <= 4096);
+  static constexpr bool TW_SMEM = (M <= 2048);
   static constexpr int TWC = tw_count(LOG2M);
   static constexpr int TWN = M / 2;
 };
 
 int stage_twiddle_count(int log2n) { return log2n >= 5 ? tw_count(log2n - 1) : 0; }
 
-int frames_per_tile(int log2n) {
+template <int LOG2N>
+struct Frames;  // frames per CTA tile
+template <> struct Frames<5> { static constexpr int F = 128; };
+template <> struct Frames<6> { static constexpr int F = 64; };
+template <> struct Frames<7> { static constexpr int F = 32; };
+template <> struct Frames<8> { static constexpr int F = 32; };
+template <> struct Frames<9> { static constexpr int F = 16; };
+template <> struct Frames<10> { static constexpr int F = 8; };
+template <> struct Frames<11> { static constexpr int F = 8; };
+template <> struct Frames<12> { static constexpr int F = 4; };
+template <> struct Frames<13> { static constexpr int F = 2; };
+template <> struct Frames<14> { static constexpr int F = 1; };
+template <> struct Frames<15> { static constexpr int F = 1; };
+
+// Launch variants of the frame kernel (picked per n_fft by the autotuner):
+//   V0: the default tile, 1024 threads' worth of registers per SM (<= 64 regs);
+//   V1: 256-thread CTAs, 3 per SM (<= 85 regs);  V2: 256-thread CTAs, 2 per SM (<= 128 regs).
+template <int LOG2N, int V>
+struct Cfg {
+  static constexpr int TPF = Shape<LOG2N>::TPF;
+  static constexpr int F = V == 0 ? Frames<LOG2N>::F : (TPF >= 256 ? 1 : 256 / TPF);
+  static constexpr int THREADS = TPF * F;
+  static constexpr int BUDGET = V == 0 ? 1024 : (V == 1 ? 768 : 512);
+  static constexpr int MINB = BUDGET / THREADS > 0 ? BUDGET / THREADS : 1;
+};
+
+__host__ __device__ constexpr bool tunable(int log2n, int mode, int pw) {
+  return (mode == MODE_MELDB || (mode == MODE_MEL && pw == 0)) && log2n >= 8 && log2n <= 13;
+}
+
+int frame_variants(int log2n, int mode, int power_is_2) {
+  return tunable(log2n, mode, power_is_2 ? 0 : 1) ? 3 : 1;
+}
+
+template <int LOG2N>
+static int frames_for(int v) {
+  return v == 1 ? Cfg<LOG2N, 1>::F : (v == 2 ? Cfg<LOG2N, 2>::F : Cfg<LOG2N, 0>::F);
+}
+
+int frames_per_tile(int log2n, int variant) {
   switch (log2n) {
-    case 5: return 128;
-    case 6: return 64;
-    case 7: return 32;
-    case 8: return 32;
-    case 9: return 16;
-    case 10: return 8;
-    case 11: return 4;
-    case 12: return 2;
-    case 13: case 14: case 15: return 1;
+    case 5: return frames_for<5>(variant);
+    case 6: return frames_for<6>(variant);
+    case 7: return frames_for<7>(variant);
+    case 8: return frames_for<8>(variant);
+    case 9: return frames_for<9>(variant);
+    case 10: return frames_for<10>(variant);
+    case 11: return frames_for<11>(variant);
+    case 12: return frames_for<12>(variant);
+    case 13: return frames_for<13>(variant);
+    case 14: return frames_for<14>(variant);
+    case 15: return frames_for<15>(variant);
     default: return 128;  // tiny kernel (n_fft <= 16)
   }
 }
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
+// Packed mel weights are staged in shared memory up to this size.
+constexpr int kMelSmemMax = 12288;  // floats
+
+// Dynamic shared memory layout of frontend_kernel (host and device agree):
+//   [mel_info n_mels x int4][mel weights][red 32 f][bad F i][tws][twn][buf F x FSTRIDE cpx]
 template <int LOG2N, int F>
 __host__ __device__ constexpr size_t fixed_smem_bytes() {
   using S = Shape<LOG2N>;
@@ -150,77 +236,43 @@ __host__ __device__ constexpr size_t fixed_smem_bytes() {
          (S::TW_SMEM ? align16(size_t(S::TWC) * 8) + align16(size_t(S::TWN) * 8) : 0) +
          size_t(F) * S::FSTRIDE * 8;
 }
-
-// ---------------------------------------------------------------------------
-// epilogue (shared by the FFT kernels): P holds |X|^power for F frames
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float mel_dot(int4 info, const float *__restrict__ w, const float *P,
-                                         bool bad) {
-  const float *wr = w + info.z;
-  const float *pr = P + info.x;
-  float acc = 0.0f;
-  for (int q = 0; q < info.y; q++) acc = fmaf(__ldg(wr + q), pr[q], acc);
-  if (info.w || bad) acc = __int_as_float(0x7fc00000);
-  return acc;
+__host__ __device__ inline size_t mel_smem_bytes(int n_mels, int nnz) {
+  return 16 * (size_t)n_mels + (nnz <= kMelSmemMax ? align16(4 * (size_t)nnz) : 0);
 }
 
-template <int MODE, int F, int THREADS>
-__device__ __forceinline__ void epilogue(const FrontArgs &a, const float *P0, int fstride, int nfreq,
-                                         const int *bad_s, const ClipDesc &cd, int c, int t0,
-                                         const int4 *mel_s, float *red_s) {
-  const int tid = threadIdx.x;
-  const long long T = cd.n_frames;
-  if constexpr (MODE == MODE_SPECTRUM) {
-    for (int it = tid; it < F * nfreq; it += THREADS) {
-      const int fi = it % F, k = it / F;
-      const int t = t0 + fi;
-      if (t < cd.n_frames) a.out[cd.out_off + (long long)k * T + t] = P0[fi * fstride + k];
-    }
-  } else if constexpr (MODE == MODE_MEL) {
-    for (int it = tid; it < F * a.n_mels; it += THREADS) {
-      const int fi = it % F, m = it / F;
-      const int t = t0 + fi;
-      if (t >= cd.n_frames) continue;
-      float acc = mel_dot(mel_s[m], a.mel_w, P0 + fi * fstride, bad_s[fi] != 0);
-      a.out[cd.out_off + (long long)m * T + t] = acc;
-    }
-  } else {
-    float vmax = -INFINITY;
-    for (int it = tid; it < F * a.n_mels; it += THREADS) {
-      const int fi = it / a.n_mels, m = it - fi * a.n_mels;
-      const int t = t0 + fi;
-      if (t >= cd.n_frames) continue;
-      float acc = mel_dot(mel_s[m], a.mel_w, P0 + fi * fstride, bad_s[fi] != 0);
-      float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
-      a.out[(cd.frame_off + t) * (long long)a.n_mels + m] = v;
-      vmax = fmaxf(vmax, v);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
-    if ((tid & 31) == 0) red_s[tid >> 5] = vmax;
-    __syncthreads();
-    if (tid < 32) {
-      float v = (tid < (THREADS + 31) / 32) ? red_s[tid] : -INFINITY;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if (tid == 0 && v > -INFINITY) atomicMax(a.clip_max + c, enc_f(v));
-    }
+// Dot product of one packed mel row with a power spectrum.
+__device__ __forceinline__ float mel_dot(int4 info, const float *w, const float *P, bool bad) {
+  const float *wr = w + info.z;
+  const float *pr = P + info.x;
+  float a0 = 0.0f, a1 = 0.0f;
+  int q = 0;
+  for (; q + 1 < info.y; q += 2) {
+    a0 = fmaf(wr[q], pr[q], a0);
+    a1 = fmaf(wr[q + 1], pr[q + 1], a1);
   }
+  if (q < info.y) a0 = fmaf(wr[q], pr[q], a0);
+  float acc = a0 + a1;
+  if (info.w || bad) acc = __int_as_float(0x7fc00000);
+  return acc;
 }
 
 // ---------------------------------------------------------------------------
 // main frame kernel, n_fft = 2^LOG2N with LOG2N in [5, 15]
 // ---------------------------------------------------------------------------
-template <int LOG2N, int F, int MODE>
-__global__ void __launch_bounds__(Shape<LOG2N>::TPF * F, (1024 / (Shape<LOG2N>::TPF * F)) > 0 ? (1024 / (Shape<LOG2N>::TPF * F)) : 1)
+template <int LOG2N, int V, int MODE, int PW>
+__global__ void __launch_bounds__(Cfg<LOG2N, V>::THREADS, Cfg<LOG2N, V>::MINB)
 frontend_kernel(FrontArgs a) {
   using S = Shape<LOG2N>;
+  constexpr int F = Cfg<LOG2N, V>::F;
   constexpr int N = S::N, M = S::M, TPF = S::TPF, THREADS = TPF * F;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int nmel_s = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  const int nmel = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  const bool mel_in_smem = (MODE != MODE_SPECTRUM) && a.mel_nnz <= kMelSmemMax;
   unsigned char *sp = smem;
   int4 *mel_s = reinterpret_cast<int4 *>(sp);
-  sp += 16 * (size_t)nmel_s;
+  sp += 16 * (size_t)nmel;
+  float *melw_s = reinterpret_cast<float *>(sp);
+  if (mel_in_smem) sp += align16(4 * (size_t)a.mel_nnz);
   float *red_s = reinterpret_cast<float *>(sp);
   sp += 128;
   int *bad_s = reinterpret_cast<int *>(sp);
@@ -239,18 +291,26 @@ frontend_kernel(FrontArgs a) {
     for (int i = tid; i < S::TWC; i += THREADS) tws_s[i] = ldc(a.tw_stage + i);
     for (int i = tid; i < S::TWN; i += THREADS) twn_s[i] = ldc(a.tw_split + i);
   }
-  for (int i = tid; i < nmel_s; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  for (int i = tid; i < nmel; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  if (mel_in_smem)
+    for (int i = tid; i < a.mel_nnz; i += THREADS) melw_s[i] = __ldg(a.mel_pw + i);
   const cpx *tws = S::TW_SMEM ? tws_s : reinterpret_cast<const cpx *>(a.tw_stage);
   const cpx *twn = S::TW_SMEM ? twn_s : reinterpret_cast<const cpx *>(a.tw_split);
+  const float *melw = mel_in_smem ? melw_s : a.mel_pw;
   __syncthreads();
 
   cpx *fb = buf + f * S::FSTRIDE;
+  float *P = reinterpret_cast<float *>(fb);
 
   for (int tile = blockIdx.x; tile < a.total_tiles; tile += gridDim.x) {
     const int c = __ldg(a.tile_clip + tile);
     const ClipDesc cd = load_clip(a.clips + c);
     const int t0 = (tile - cd.tile_base) * F;
-    const long long s0 = (long long)(t0 + f) * a.hop - a.pad;
+    const int t = t0 + f;
+    // Log-mel frame groups that fill whole warps work independently: an
+    // out-of-range frame skips the tile (its group's barriers are its own).
+    if (MODE == MODE_MELDB && TPF >= 32 && t >= cd.n_frames) continue;
+    const long long s0 = (long long)t * a.hop - a.pad;
     const float *sig = a.signal + cd.sig_off;
 
     // ---- gather: z[n] = (x[2n] w[2n], x[2n+1] w[2n+1]) for n = j + r*M/16
@@ -284,11 +344,10 @@ frontend_kernel(FrontArgs a) {
 
     // ---- stage 0: radix 16, Ns = 1 (no twiddles)
     dft16(v);
-    __syncthreads();  // the previous tile's epilogue has finished with buf / bad_s
-    if (j == 0) bad_s[f] = 0;
+    frame_sync<TPF>(f);  // the previous tile's epilogue has finished with fb
 #pragma unroll
     for (int r = 0; r < 16; r++) fb[padx(j * 16 + r)] = v[r];
-    __syncthreads();
+    frame_sync<TPF>(f);
 
     // ---- radix-16 stages 1 .. N16-1
 #pragma unroll
@@ -301,11 +360,11 @@ frontend_kernel(FrontArgs a) {
 #pragma unroll
       for (int r = 1; r < 16; r++) v[r] = cmul(v[r], tw[(r - 1) * Ns]);
       dft16(v);
-      __syncthreads();
+      frame_sync<TPF>(f);
       const int base = (j - k) * 16 + k;
 #pragma unroll
       for (int r = 0; r < 16; r++) fb[padx(base + r * Ns)] = v[r];
-      __syncthreads();
+      frame_sync<TPF>(f);
     }
 
     // ---- trailing radix-R stage (in place: each thread rewrites what it read)
@@ -323,7 +382,7 @@ frontend_kernel(FrontArgs a) {
 #pragma unroll
         for (int qq = 0; qq < R; qq++) fb[padx(b + qq * Ns)] = v[i * R + qq];
       }
-      __syncthreads();
+      frame_sync<TPF>(f);
     }
 
     // ---- real split: X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
@@ -352,45 +411,85 @@ frontend_kernel(FrontArgs a) {
       const cpx z = fb[padx(M / 2)];
       pmid = z.x * z.x + z.y * z.y;
     }
-    __syncthreads();
-    float *P = reinterpret_cast<float *>(fb);
-    bool nonfinite = false;
+    frame_sync<TPF>(f);
+    float chk = 0.0f;  // sum of this thread's |X|^power: non-finite iff one term is
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int k = j + i * TPF;
-      const float x = apply_power(pa[i], a.power);
-      const float y = apply_power(pb[i], a.power);
+      const float x = apply_power<PW>(pa[i], a.power);
+      const float y = apply_power<PW>(pb[i], a.power);
       P[k] = x;
       P[M - k] = y;
-      nonfinite |= !(isfinite(x) && isfinite(y));
+      chk += x + y;
     }
     if (j == 0) {
-      const float x = apply_power(pmid, a.power);
+      const float x = apply_power<PW>(pmid, a.power);
       P[M / 2] = x;
-      nonfinite |= !isfinite(x);
+      chk += x;
     }
-    if (MODE != MODE_SPECTRUM && nonfinite) bad_s[f] = 1;
-    __syncthreads();
+    const bool bad = frame_sync_or<TPF>(f, !isfinite(chk));
 
-    epilogue<MODE, F, THREADS>(a, reinterpret_cast<const float *>(buf), 2 * S::FSTRIDE, M + 1,
-                               bad_s, cd, c, t0, mel_s, red_s);
+    if constexpr (MODE == MODE_MELDB) {
+      // frame-local epilogue: log-mel row of this frame + running clip max
+      const bool valid = t < cd.n_frames;
+      float vmax = -INFINITY;
+      float *dst = a.out + (cd.frame_off + t) * (long long)a.n_mels;
+      for (int m = j; m < a.n_mels; m += TPF) {
+        const float acc = mel_dot(mel_s[m], melw, P, bad);
+        const float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        if (valid) dst[m] = v;
+        vmax = fmaxf(vmax, v);
+      }
+      if (!valid) vmax = -INFINITY;
+      constexpr int W = TPF < 32 ? TPF : 32;
+#pragma unroll
+      for (int o = W / 2; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+      if ((j & (W - 1)) == 0 && vmax > -INFINITY) atomicMax(a.clip_max + c, enc_f(vmax));
+    } else {
+      // CTA-wide epilogues write [rows][T] blocks: F consecutive frames per row
+      if (j == 0) bad_s[f] = bad ? 1 : 0;
+      __syncthreads();
+      const long long T = cd.n_frames;
+      const float *P0 = reinterpret_cast<const float *>(buf);
+      constexpr int FS = 2 * S::FSTRIDE;
+      if constexpr (MODE == MODE_SPECTRUM) {
+        for (int it = tid; it < F * (M + 1); it += THREADS) {
+          const int fi = it % F, k = it / F;
+          const int tt = t0 + fi;
+          if (tt < cd.n_frames) a.out[cd.out_off + (long long)k * T + tt] = P0[fi * FS + k];
+        }
+      } else {
+        for (int it = tid; it < F * a.n_mels; it += THREADS) {
+          const int fi = it % F, m = it / F;
+          const int tt = t0 + fi;
+          if (tt >= cd.n_frames) continue;
+          a.out[cd.out_off + (long long)m * T + tt] = mel_dot(mel_s[m], melw, P0 + fi * FS, bad_s[fi] != 0);
+        }
+      }
+      __syncthreads();  // the next tile overwrites buf
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
 // tiny frames (n_fft <= 16): direct DFT, one thread per frame
 // ---------------------------------------------------------------------------
-template <int MODE>
+template <int MODE, int PW>
 __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_fft) {
   constexpr int F = 128, THREADS = 128, PST = 9;
   __shared__ float P_s[F * PST];
   __shared__ int bad_s[F];
   __shared__ float red_s[32];
   extern __shared__ __align__(16) unsigned char smem[];
+  const int nmel = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
   int4 *mel_s = reinterpret_cast<int4 *>(smem);
-  const int nmel_s = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  float *melw_s = reinterpret_cast<float *>(smem + 16 * (size_t)nmel);
+  const bool mel_in_smem = (MODE != MODE_SPECTRUM) && a.mel_nnz <= kMelSmemMax;
   const int tid = threadIdx.x;
-  for (int i = tid; i < nmel_s; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  for (int i = tid; i < nmel; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
+  if (mel_in_smem)
+    for (int i = tid; i < a.mel_nnz; i += THREADS) melw_s[i] = __ldg(a.mel_pw + i);
+  const float *melw = mel_in_smem ? melw_s : a.mel_pw;
   const int nfreq = n_fft / 2 + 1;
   for (int tile = blockIdx.x; tile < a.total_tiles; tile += gridDim.x) {
     const int c = __ldg(a.tile_clip + tile);
@@ -403,7 +502,7 @@ __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_f
     for (int n = 0; n < 16; n++)
       xw[n] = (n < n_fft) ? sample_at(sig, s0 + n, cd.length, a.pad_mode) * __ldg(a.window + n) : 0.0f;
     float p[PST];
-    bool nonfinite = false;
+    float chk = 0.0f;
 #pragma unroll
     for (int k = 0; k < PST; k++) {
       float re = 0.0f, im = 0.0f;
@@ -414,63 +513,121 @@ __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_f
           im = fmaf(xw[n], w.y, im);
         }
       }
-      p[k] = apply_power(re * re + im * im, a.power);
-      if (k < nfreq) nonfinite |= !isfinite(p[k]);
+      p[k] = apply_power<PW>(re * re + im * im, a.power);
+      if (k < nfreq) chk += p[k];
     }
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < PST; k++) P_s[tid * PST + k] = p[k];
-    bad_s[tid] = (MODE != MODE_SPECTRUM && nonfinite) ? 1 : 0;
+    bad_s[tid] = !isfinite(chk);
     __syncthreads();
-    epilogue<MODE, F, THREADS>(a, P_s, PST, nfreq, bad_s, cd, c, t0, mel_s, red_s);
+    const long long T = cd.n_frames;
+    if constexpr (MODE == MODE_SPECTRUM) {
+      for (int it = tid; it < F * nfreq; it += THREADS) {
+        const int fi = it % F, k = it / F;
+        const int tt = t0 + fi;
+        if (tt < cd.n_frames) a.out[cd.out_off + (long long)k * T + tt] = P_s[fi * PST + k];
+      }
+    } else if constexpr (MODE == MODE_MEL) {
+      for (int it = tid; it < F * a.n_mels; it += THREADS) {
+        const int fi = it % F, m = it / F;
+        const int tt = t0 + fi;
+        if (tt < cd.n_frames)
+          a.out[cd.out_off + (long long)m * T + tt] = mel_dot(mel_s[m], melw, P_s + fi * PST, bad_s[fi] != 0);
+      }
+    } else {
+      float vmax = -INFINITY;
+      for (int it = tid; it < F * a.n_mels; it += THREADS) {
+        const int fi = it / a.n_mels, m = it - fi * a.n_mels;
+        const int tt = t0 + fi;
+        if (tt >= cd.n_frames) continue;
+        const float acc = mel_dot(mel_s[m], melw, P_s + fi * PST, bad_s[fi] != 0);
+        const float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        a.out[(cd.frame_off + tt) * (long long)a.n_mels + m] = v;
+        vmax = fmaxf(vmax, v);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+      if ((tid & 31) == 0) red_s[tid >> 5] = vmax;
+      __syncthreads();
+      if (tid < 32) {
+        float v = (tid < THREADS / 32) ? red_s[tid] : -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (tid == 0 && v > -INFINITY) atomicMax(a.clip_max + c, enc_f(v));
+      }
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// clamp (top_db floor) + DCT-II over the frame-major log-mel
+// top_db floor + DCT-II over the frame-major log-mel: per tile of 64 frames of
+// one clip, out[k][t] = sum_n B[k][n] * max(D[t][n], max_db - top_db).
+// 256 threads = 64 frames x 4 coefficient groups of KQ coefficients each.
 // ---------------------------------------------------------------------------
+constexpr int kDctMC = 64;        // mel chunk
+constexpr int kDctTS = kDctMC + 4;  // tile row stride (floats): float4 rows, conflict-free
+constexpr int kDctKC = 32;        // coefficient chunk
+
+template <int KQ>
 __global__ void __launch_bounds__(256) dct_kernel(DctArgs a) {
-  constexpr int TT = kDctTile, MC = 128;
-  __shared__ float tile[TT][MC + 1];
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  constexpr int TT = kDctTile;
+  __shared__ __align__(16) float tile[TT * kDctTS];
+  __shared__ __align__(16) float bas[4 * KQ * kDctMC];
+  const int tid = threadIdx.x;
+  const int fr = tid & (TT - 1), kg = tid / TT;
   for (int ti = blockIdx.x; ti < a.total_tiles; ti += gridDim.x) {
     const int c = __ldg(a.tile_clip + ti);
     const ClipDesc cd = load_clip(a.clips + c);
     const int tf = __ldg(a.tile_first + ti);
     const int nt = min(TT, cd.n_frames - tf);
-    const float thr = (a.top_db > 0.0f) ? dec_f(__ldg(a.clip_max + c)) - a.top_db : -INFINITY;
+    const bool floor_on = a.top_db > 0.0f;
+    const float thr = floor_on ? dec_f(__ldg(a.clip_max + c)) - a.top_db : 0.0f;
     const float *src = a.mel_db + (cd.frame_off + tf) * (long long)a.n_mels;
     const long long T = cd.n_frames;
-    for (int kc = 0; kc < a.n_mfcc; kc += 32) {
-      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-      for (int mc = 0; mc < a.n_mels; mc += MC) {
-        const int mw = min(MC, a.n_mels - mc);
+    for (int kc = 0; kc < a.n_mfcc; kc += 4 * KQ) {
+      float acc[KQ];
+#pragma unroll
+      for (int q = 0; q < KQ; q++) acc[q] = 0.0f;
+      for (int mc = 0; mc < a.n_mels; mc += kDctMC) {
+        const int mw = min(kDctMC, a.n_mels - mc);
         __syncthreads();
-        for (int i = tid; i < TT * MC; i += 256) {
-          const int r = i / MC, col = i - r * MC;
+        for (int i = tid; i < TT * kDctMC; i += 256) {
+          const int r = i / kDctMC, col = i - r * kDctMC;
           float x = 0.0f;
           if (r < nt && col < mw) {
             x = __ldg(src + (long long)r * a.n_mels + mc + col);
-            if (a.top_db > 0.0f) x = vthr(x, thr);
+            if (floor_on) x = vthr(x, thr);
           }
-          tile[r][col] = x;
+          tile[r * kDctTS + col] = x;
+        }
+        for (int i = tid; i < 4 * KQ * kDctMC; i += 256) {
+          const int k = i / kDctMC, col = i - k * kDctMC;
+          const int kk = kc + k;
+          bas[i] = (kk < a.n_mfcc && col < mw) ? __ldg(a.basis + (long long)kk * a.n_mels + mc + col) : 0.0f;
         }
         __syncthreads();
+        const float4 *trow = reinterpret_cast<const float4 *>(tile + fr * kDctTS);
+        const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * kDctMC);
+#pragma unroll 4
+        for (int n4 = 0; n4 < kDctMC / 4; n4++) {
+          const float4 d = trow[n4];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          const int k = kc + w + 8 * q;
-          if (k < a.n_mfcc) {
-            const float *brow = a.basis + (long long)k * a.n_mels + mc;
-            float s = acc[q];
-            for (int n = 0; n < mw; n++) s = fmaf(__ldg(brow + n), tile[lane][n], s);
-            acc[q] = s;
+          for (int q = 0; q < KQ; q++) {
+            const float4 b = brow[q * (kDctMC / 4) + n4];
+            acc[q] = fmaf(b.x, d.x, acc[q]);
+            acc[q] = fmaf(b.y, d.y, acc[q]);
+            acc[q] = fmaf(b.z, d.z, acc[q]);
+            acc[q] = fmaf(b.w, d.w, acc[q]);
           }
         }
       }
+      if (fr < nt) {
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int k = kc + w + 8 * q;
-        if (k < a.n_mfcc && lane < nt) a.out[cd.out_off + (long long)k * T + tf + lane] = acc[q];
+        for (int q = 0; q < KQ; q++) {
+          const int k = kc + kg * KQ + q;
+          if (k < a.n_mfcc) a.out[cd.out_off + (long long)k * T + tf + fr] = acc[q];
+        }
       }
     }
   }
@@ -506,6 +663,16 @@ __global__ void __launch_bounds__(256) db_pass2_kernel(float *y, long long n, fl
   const float thr = dec_f(*slot) - top_db;
   for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256)
     y[i] = vthr(y[i], thr);
+}
+
+__global__ void fill_pattern_kernel(float *p, long long n) {
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    unsigned h = (unsigned)i * 2654435761u;
+    h ^= h >> 16;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    p[i] = (float)(h & 0xffffff) / 16777216.0f - 0.5f;
+  }
 }
 
 __global__ void fill_u32_kernel(unsigned *p, unsigned v, long long n) {
@@ -580,7 +747,7 @@ __global__ void build_mel_kernel(float *W, int sr, int n_fft, int n_mels, double
   W[i] = (float)(w * enorm);
 }
 
-// Per-mel nonzero range of the dense filterbank + NaN-row flag.
+// Per-mel nonzero range of the dense filterbank + NaN-row flag (z = count for now).
 __global__ void build_mel_info_kernel(int4 *info, const float *W, int n_mels, int nfreq) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= n_mels) return;
@@ -594,8 +761,26 @@ __global__ void build_mel_info_kernel(int4 *info, const float *W, int n_mels, in
       last = k;
     }
   }
-  if (first < 0) info[m] = make_int4(0, 0, m * nfreq, nan_row);
-  else info[m] = make_int4(first, last - first + 1, m * nfreq + first, nan_row);
+  if (first < 0) info[m] = make_int4(0, 0, 0, nan_row);
+  else info[m] = make_int4(first, last - first + 1, 0, nan_row);
+}
+
+// Exclusive prefix sum of the row lengths into info[m].z; total into *nnz.
+__global__ void mel_offsets_kernel(int4 *info, int n_mels, int *nnz) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int off = 0;
+  for (int m = 0; m < n_mels; m++) {
+    info[m].z = off;
+    off += info[m].y;
+  }
+  *nnz = off;
+}
+
+__global__ void mel_pack_kernel(float *packed, const float *W, const int4 *info, int n_mels, int nfreq) {
+  const int m = blockIdx.x;
+  if (m >= n_mels) return;
+  const int4 in = info[m];
+  for (int q = threadIdx.x; q < in.y; q += blockDim.x) packed[in.z + q] = W[(long long)m * nfreq + in.x + q];
 }
 
 // DCT-II ortho basis (MFCC.swift:79-88) in float64.
@@ -645,11 +830,22 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
   }
   if (n_mels > 0) {
     const long long cnt = (long long)n_mels * nfreq;
+    int *d_nnz = nullptr;
     MM_TRY(cudaMalloc(&t.mel_w, sizeof(float) * (size_t)cnt));
     MM_TRY(cudaMalloc(&t.mel_info, sizeof(int4) * (size_t)n_mels));
+    MM_TRY(cudaMalloc(&d_nnz, sizeof(int)));
     build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
                                                           (double)fmax);
     build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
+    mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
+    int nnz = 0;
+    e = cudaMemcpyAsync(&nnz, d_nnz, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_nnz);
+    if (e != cudaSuccess) return e;
+    t.mel_nnz = nnz;
+    MM_TRY(cudaMalloc(&t.mel_pw, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)));
+    mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
   }
   if (n_mfcc_eff > 0 && n_mels > 0) {
     MM_TRY(cudaMalloc(&t.dct, sizeof(float) * (size_t)n_mfcc_eff * n_mels));
@@ -660,90 +856,123 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
   return cudaGetLastError();
 }
 
-template <int LOG2N, int F, int MODE>
-static cudaError_t launch_fft_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
-  using S = Shape<LOG2N>;
-  constexpr int THREADS = S::TPF * F;
-  const size_t smem = fixed_smem_bytes<LOG2N, F>() + (MODE == MODE_SPECTRUM ? 0 : 16 * (size_t)a.n_mels);
-  auto kern = frontend_kernel<LOG2N, F, MODE>;
-  static size_t configured = 0;
-  cudaError_t e;
-  if (smem > 48 * 1024 && smem > configured) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = smem;
-  }
-  int dev = 0, sms = 148, per_sm = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem);
-  if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  long long grid = (long long)sms * per_sm;
-  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
-  if (grid > a.total_tiles) grid = a.total_tiles;
-  if (grid < 1) return cudaSuccess;
-  kern<<<(unsigned)grid, THREADS, smem, s>>>(a);
-  if (launched) *launched = (int)grid;
-  return cudaGetLastError();
-}
-
-template <int MODE>
-static cudaError_t launch_mode(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
-  switch (log2n) {
-    case 5: return launch_fft_t<5, 128, MODE>(a, grid_limit, s, launched);
-    case 6: return launch_fft_t<6, 64, MODE>(a, grid_limit, s, launched);
-    case 7: return launch_fft_t<7, 32, MODE>(a, grid_limit, s, launched);
-    case 8: return launch_fft_t<8, 32, MODE>(a, grid_limit, s, launched);
-    case 9: return launch_fft_t<9, 16, MODE>(a, grid_limit, s, launched);
-    case 10: return launch_fft_t<10, 8, MODE>(a, grid_limit, s, launched);
-    case 11: return launch_fft_t<11, 4, MODE>(a, grid_limit, s, launched);
-    case 12: return launch_fft_t<12, 2, MODE>(a, grid_limit, s, launched);
-    case 13: return launch_fft_t<13, 1, MODE>(a, grid_limit, s, launched);
-    case 14: return launch_fft_t<14, 1, MODE>(a, grid_limit, s, launched);
-    case 15: return launch_fft_t<15, 1, MODE>(a, grid_limit, s, launched);
-    default: break;
-  }
-  if (log2n < 0 || log2n > 4) return cudaErrorInvalidValue;
-  const size_t smem = (MODE == MODE_SPECTRUM) ? 0 : 16 * (size_t)a.n_mels;
-  auto kern = frontend_tiny_kernel<MODE>;
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-  }
+static int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long grid = (long long)sms * 4;
+  return sms;
+}
+
+template <bool TINY, typename K>
+static cudaError_t launch_persistent(K kern, int threads, size_t smem, int tiles, int grid_limit,
+                                     size_t *configured, const FrontArgs &a, cudaStream_t s,
+                                     int *launched, int n_fft) {
+  cudaError_t e;
+  if (smem > 48 * 1024 && smem > *configured) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    *configured = smem;
+  }
+  int per_sm = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  long long grid = (long long)sm_count() * per_sm;
   if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
-  if (grid > a.total_tiles) grid = a.total_tiles;
+  if (grid > tiles) grid = tiles;
   if (grid < 1) return cudaSuccess;
-  kern<<<(unsigned)grid, 128, smem, s>>>(a, 1 << log2n);
+  if constexpr (TINY) kern<<<(unsigned)grid, threads, smem, s>>>(a, n_fft);
+  else kern<<<(unsigned)grid, threads, smem, s>>>(a);
   if (launched) *launched = (int)grid;
   return cudaGetLastError();
 }
 
-cudaError_t launch_frontend(int log2n, int mode, const FrontArgs &a, int grid_limit, cudaStream_t s,
-                            int *launched) {
+template <int LOG2N, int V, int MODE, int PW>
+static cudaError_t launch_fft_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  using C = Cfg<LOG2N, V>;
+  const size_t smem = fixed_smem_bytes<LOG2N, C::F>() +
+                      (MODE == MODE_SPECTRUM ? 0 : mel_smem_bytes(a.n_mels, a.mel_nnz));
+  static size_t configured = 0;
+  return launch_persistent<false>(frontend_kernel<LOG2N, V, MODE, PW>, C::THREADS, smem, a.total_tiles,
+                                  grid_limit, &configured, a, s, launched, 1 << LOG2N);
+}
+
+template <int LOG2N, int MODE, int PW>
+static cudaError_t launch_size(int v, const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  if constexpr (tunable(LOG2N, MODE, PW)) {
+    if (v == 1) return launch_fft_t<LOG2N, 1, MODE, PW>(a, grid_limit, s, launched);
+    if (v == 2) return launch_fft_t<LOG2N, 2, MODE, PW>(a, grid_limit, s, launched);
+  }
+  return launch_fft_t<LOG2N, 0, MODE, PW>(a, grid_limit, s, launched);
+}
+
+template <int MODE, int PW>
+static cudaError_t launch_mode(int log2n, int v, const FrontArgs &a, int grid_limit, cudaStream_t s,
+                               int *launched) {
+  switch (log2n) {
+    case 5: return launch_size<5, MODE, PW>(v, a, grid_limit, s, launched);
+    case 6: return launch_size<6, MODE, PW>(v, a, grid_limit, s, launched);
+    case 7: return launch_size<7, MODE, PW>(v, a, grid_limit, s, launched);
+    case 8: return launch_size<8, MODE, PW>(v, a, grid_limit, s, launched);
+    case 9: return launch_size<9, MODE, PW>(v, a, grid_limit, s, launched);
+    case 10: return launch_size<10, MODE, PW>(v, a, grid_limit, s, launched);
+    case 11: return launch_size<11, MODE, PW>(v, a, grid_limit, s, launched);
+    case 12: return launch_size<12, MODE, PW>(v, a, grid_limit, s, launched);
+    case 13: return launch_size<13, MODE, PW>(v, a, grid_limit, s, launched);
+    case 14: return launch_size<14, MODE, PW>(v, a, grid_limit, s, launched);
+    case 15: return launch_size<15, MODE, PW>(v, a, grid_limit, s, launched);
+    default: break;
+  }
+  if (log2n < 0 || log2n > 4) return cudaErrorInvalidValue;
+  const size_t smem = (MODE == MODE_SPECTRUM) ? 0 : mel_smem_bytes(a.n_mels, a.mel_nnz);
+  static size_t configured = 0;
+  return launch_persistent<true>(frontend_tiny_kernel<MODE, PW>, 128, smem, a.total_tiles, grid_limit,
+                                 &configured, a, s, launched, 1 << log2n);
+}
+
+cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,
+                            cudaStream_t s, int *launched) {
   if (launched) *launched = 0;
   if (a.total_tiles <= 0) return cudaSuccess;
+  const int pw = (a.power == 2.0f) ? 0 : (a.power == 1.0f ? 1 : 2);
   switch (mode) {
-    case MODE_SPECTRUM: return launch_mode<MODE_SPECTRUM>(log2n, a, grid_limit, s, launched);
-    case MODE_MEL: return launch_mode<MODE_MEL>(log2n, a, grid_limit, s, launched);
-    case MODE_MELDB: return launch_mode<MODE_MELDB>(log2n, a, grid_limit, s, launched);
+    case MODE_SPECTRUM:
+      if (pw == 0) return launch_mode<MODE_SPECTRUM, 0>(log2n, variant, a, grid_limit, s, launched);
+      if (pw == 1) return launch_mode<MODE_SPECTRUM, 1>(log2n, variant, a, grid_limit, s, launched);
+      return launch_mode<MODE_SPECTRUM, 2>(log2n, variant, a, grid_limit, s, launched);
+    case MODE_MEL:
+      if (pw == 0) return launch_mode<MODE_MEL, 0>(log2n, variant, a, grid_limit, s, launched);
+      if (pw == 1) return launch_mode<MODE_MEL, 1>(log2n, variant, a, grid_limit, s, launched);
+      return launch_mode<MODE_MEL, 2>(log2n, variant, a, grid_limit, s, launched);
+    case MODE_MELDB:
+      if (pw != 0) return cudaErrorInvalidValue;
+      return launch_mode<MODE_MELDB, 0>(log2n, variant, a, grid_limit, s, launched);
     default: return cudaErrorInvalidValue;
   }
 }
 
+template <int KQ>
+static cudaError_t launch_dct_t(const DctArgs &a, cudaStream_t s) {
+  long long grid = (long long)sm_count() * 4;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  dct_kernel<KQ><<<(unsigned)grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long grid = (long long)sms * 8;
-  if (grid > a.total_tiles) grid = a.total_tiles;
-  dct_kernel<<<(unsigned)grid, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  // 4 coefficient groups x KQ accumulators cover min(n_mfcc, 32) coefficients per pass
+  const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
+  switch (kq) {
+    case 1: return launch_dct_t<1>(a, s);
+    case 2: return launch_dct_t<2>(a, s);
+    case 3: return launch_dct_t<3>(a, s);
+    case 4: return launch_dct_t<4>(a, s);
+    case 5: return launch_dct_t<5>(a, s);
+    case 6: return launch_dct_t<6>(a, s);
+    case 7: return launch_dct_t<7>(a, s);
+    default: return launch_dct_t<8>(a, s);
+  }
 }
 
 cudaError_t launch_fill_u32(unsigned *p, unsigned v, long long n, cudaStream_t s) {
@@ -751,6 +980,14 @@ cudaError_t launch_fill_u32(unsigned *p, unsigned v, long long n, cudaStream_t s
   long long g = (n + 255) / 256;
   if (g > 4096) g = 4096;
   fill_u32_kernel<<<(unsigned)g, 256, 0, s>>>(p, v, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_pattern(float *p, long long n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  long long g = (n + 255) / 256;
+  if (g > 4096) g = 4096;
+  fill_pattern_kernel<<<(unsigned)g, 256, 0, s>>>(p, n);
   return cudaGetLastError();
 }
 

@@ -31,8 +31,10 @@ struct DevTables {
   float2 *tw_stage = nullptr;  // per-stage Stockham twiddles (layout: stage_twiddle_count)
   float2 *tw_split = nullptr;  // exp(-2 pi i k / n_fft), k < n_fft/4 (real split)
   float2 *tw_tiny = nullptr;   // exp(-2 pi i t / n_fft), t < n_fft (n_fft <= 16 only)
-  float *mel_w = nullptr;      // dense [n_mels][n_fft/2+1] float32 weights
-  int4 *mel_info = nullptr;    // per mel {start bin, count, dense offset, nan-row flag}
+  float *mel_w = nullptr;      // dense [n_mels][n_fft/2+1] float32 weights (build stage)
+  float *mel_pw = nullptr;     // packed nonzero weights, row after row
+  int4 *mel_info = nullptr;    // per mel {start bin, count, packed offset, nan-row flag}
+  int mel_nnz = 0;             // entries of mel_pw
   float *dct = nullptr;        // [n_mfcc_eff][n_mels] DCT-II ortho basis
 };
 
@@ -47,7 +49,8 @@ struct FrontArgs {
   const float2 *tw_split;
   const float2 *tw_tiny;
   const int4 *mel_info;
-  const float *mel_w;
+  const float *mel_pw;  // packed weights (mel_info[m].z = offset of row m)
+  int mel_nnz;
   int n_mels;
   float power;  // exponent applied to |X| (2 = power spectrum)
   float amin, ref;
@@ -68,10 +71,12 @@ struct DctArgs {
   float *out;    // per clip [n_mfcc][n_frames] at clips[c].out_off
 };
 
-constexpr int kDctTile = 32;
+constexpr int kDctTile = 64;  // frames per DCT tile
 
-// Frames per CTA tile for a given log2(n_fft).
-int frames_per_tile(int log2n);
+// Frames per CTA tile for a given log2(n_fft) and launch variant.
+int frames_per_tile(int log2n, int variant);
+// Number of launch variants the autotuner may choose from (1 = not tunable).
+int frame_variants(int log2n, int mode, int power_is_2);
 // Stockham twiddle table length (entries) for log2(n_fft) >= 5.
 int stage_twiddle_count(int log2n);
 
@@ -80,10 +85,12 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
                          float fmax, int n_mfcc_eff, int window_zero, cudaStream_t s);
 
 // Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
-cudaError_t launch_frontend(int log2n, int mode, const FrontArgs &a, int grid_limit,
+cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,
                             cudaStream_t s, int *launched_grid);
 cudaError_t launch_dct(const DctArgs &a, cudaStream_t s);
 cudaError_t launch_fill_u32(unsigned *p, unsigned v, long long n, cudaStream_t s);
+// Deterministic pseudo-random samples in [-0.5, 0.5) (autotuning inputs).
+cudaError_t launch_fill_pattern(float *p, long long n, cudaStream_t s);
 
 // dB scaling over a flat array: pass 1 writes mult*log10(max(x,amin)/ref) and the
 // encoded max into *slot; pass 2 floors at max - top_db.

@@ -4,6 +4,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -30,6 +31,20 @@ int gpu_available() {
     else cudaGetLastError();
   });
   return status;
+}
+
+namespace {
+std::atomic<int> g_tuned[16];
+}
+
+int tuned_variant(int log2n) { return (log2n >= 0 && log2n < 16) ? g_tuned[log2n].load() : 0; }
+void set_tuned_variant(int log2n, int v) {
+  if (log2n >= 0 && log2n < 16) g_tuned[log2n].store(v);
+}
+int group_variant(const Group &g) {
+  const int nv = frame_variants(g.log2n, g.mode, g.power == 2.0f);
+  const int v = tuned_variant(g.log2n);
+  return (v >= 0 && v < nv) ? v : 0;
 }
 
 int is_pow2(long long n) { return n > 0 && (n & (n - 1)) == 0; }
@@ -101,6 +116,7 @@ const DevTables *get_tables(const Group &g, int *status) {
     cudaFree(t->tw_split);
     cudaFree(t->tw_tiny);
     cudaFree(t->mel_w);
+    cudaFree(t->mel_pw);
     cudaFree(t->mel_info);
     cudaFree(t->dct);
     delete t;
@@ -121,7 +137,7 @@ void make_layout(const Group &g, const int64_t *lengths, int n, Layout &L) {
   L.tile_clip.clear();
   L.dct_tile_clip.clear();
   L.dct_tile_first.clear();
-  L.F = frames_per_tile(g.log2n);
+  L.F = frames_per_tile(g.log2n, g.variant);
   const int rows = output_rows(g);
   long long sig = 0, frames = 0, out = 0;
   int tiles = 0;
@@ -234,7 +250,8 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.tw_split = t->tw_split;
   a.tw_tiny = t->tw_tiny;
   a.mel_info = t->mel_info;
-  a.mel_w = t->mel_w;
+  a.mel_pw = t->mel_pw;
+  a.mel_nnz = t->mel_nnz;
   a.n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
   a.power = g.power;
   a.amin = g.amin;
@@ -242,7 +259,7 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.out = (g.mode == MODE_MELDB) ? b.meldb : b.out;
   a.clip_max = b.clip_max;
   int grid = 0;
-  if ((e = launch_frontend(g.log2n, g.mode, a, 0, s, &grid)) != cudaSuccess) return e;
+  if ((e = launch_frontend(g.log2n, g.mode, g.variant, a, 0, s, &grid)) != cudaSuccess) return e;
   if (grid > 0) launches++;
   if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
   if (g.mode == MODE_MELDB && g.n_mfcc_eff > 0 && !L.dct_tile_clip.empty()) {

@@ -24,7 +24,14 @@ struct Group {
   int n_mels = 128, n_mfcc_eff = 20;
   float fmin = 0.0f, fmax = 11025.0f, top_db = 80.0f;
   float power = 2.0f, amin = 1e-10f, ref = 1.0f;
+  int variant = 0;  // frame-kernel launch variant (autotuned per n_fft)
 };
+
+// Process-wide autotuning table: launch variant per log2(n_fft).
+int tuned_variant(int log2n);
+void set_tuned_variant(int log2n, int v);
+// The variant a group of this mode/power/size runs with (0 when not tunable).
+int group_variant(const Group &g);
 
 int is_pow2(long long n);
 int ilog2(long long n);

@@ -270,3 +270,33 @@ def test_plan_graph_replay_and_host_io():
         for x, y_, r in zip(a, b, ref):
             np.testing.assert_array_equal(x, y_)
             np.testing.assert_array_equal(x, r)
+
+
+# ---------------------------------------------------------------------------
+# launch variants (autotuner search space): every variant is parity-checked
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("n_fft", [256, 512, 1024, 2048, 4096, 8192])
+def test_every_launch_variant_vs_oracle(n_fft):
+    y = synth.music_clip(3 * 22050 + 123, SR, seed=n_fft)
+    exp = O.mfcc(y, SR, 20, n_fft, n_fft // 4, n_fft, 64)
+    exp_mel = O.melspectrogram(y, SR, n_fft, n_fft // 4, n_fft, True, 2.0, 64)
+    old = M.tune_get(n_fft)
+    try:
+        for v in range(3):
+            M.tune_set(n_fft, v)
+            got = M.mfcc(y, sr=SR, n_fft=n_fft, hop_length=n_fft // 4, n_mels=64)
+            assert O.mfcc_rel_error(got, exp) < MFCC_TOL, (v, O.mfcc_rel_error(got, exp))
+            mel = M.melspectrogram(y, sr=SR, n_fft=n_fft, hop_length=n_fft // 4, n_mels=64)
+            assert np.abs(mel - exp_mel).max() <= 1e-5 * exp_mel.max(), v
+    finally:
+        M.tune_set(n_fft, old)
+
+
+def test_autotune_picks_a_variant_and_keeps_parity():
+    res = M.autotune(clip_samples=22050 * 5, n_clips=8, reps=3, sr=SR, n_fft=2048, hop_length=512)
+    assert res["best"] in (0, 1, 2) and len(res["ms"]) == 3 and all(m > 0 for m in res["ms"])
+    assert M.tune_get(2048) == res["best"]
+    y = synth.music_clip(22050 * 4, SR, seed=9)
+    got = M.mfcc(y, sr=SR)
+    assert O.mfcc_rel_error(got, O.mfcc(y, SR, 20, 2048, 512, 2048, 128)) < MFCC_TOL

@@ -584,6 +584,7 @@ __global__ void __launch_bounds__(256) dct_kernel(DctArgs a) {
     const bool floor_on = a.top_db > 0.0f;
     const float thr = floor_on ? dec_f(__ldg(a.clip_max + c)) - a.top_db : 0.0f;
     const float *src = a.mel_db + (cd.frame_off + tf) * (long long)a.n_mels;
+    const bool vec4 = (a.n_mels & 3) == 0;  // mel_db is 256-byte aligned, rows n_mels floats
     const long long T = cd.n_frames;
     for (int kc = 0; kc < a.n_mfcc; kc += 4 * KQ) {
       float acc[KQ];
@@ -592,14 +593,46 @@ __global__ void __launch_bounds__(256) dct_kernel(DctArgs a) {
       for (int mc = 0; mc < a.n_mels; mc += kDctMC) {
         const int mw = min(kDctMC, a.n_mels - mc);
         __syncthreads();
-        for (int i = tid; i < TT * kDctMC; i += 256) {
-          const int r = i / kDctMC, col = i - r * kDctMC;
-          float x = 0.0f;
-          if (r < nt && col < mw) {
-            x = __ldg(src + (long long)r * a.n_mels + mc + col);
-            if (floor_on) x = vthr(x, thr);
+        if (vec4) {
+          // rows of the frame-major log-mel are 16-byte aligned: 4 float4 per thread, loads first
+          float4 x[TT * kDctMC / 4 / 256];
+#pragma unroll
+          for (int u = 0; u < TT * kDctMC / 4 / 256; u++) {
+            const int i = tid + 256 * u;
+            const int r = i / (kDctMC / 4), c4 = i - r * (kDctMC / 4);
+            x[u] = (r < nt && 4 * c4 < mw)
+                       ? __ldg(reinterpret_cast<const float4 *>(src + (long long)r * a.n_mels + mc) + c4)
+                       : make_float4(0.f, 0.f, 0.f, 0.f);
           }
-          tile[r * kDctTS + col] = x;
+#pragma unroll
+          for (int u = 0; u < TT * kDctMC / 4 / 256; u++) {
+            const int i = tid + 256 * u;
+            const int r = i / (kDctMC / 4), c4 = i - r * (kDctMC / 4);
+            float4 v = x[u];
+            if (floor_on && r < nt && 4 * c4 < mw) {
+              v.x = vthr(v.x, thr);
+              v.y = vthr(v.y, thr);
+              v.z = vthr(v.z, thr);
+              v.w = vthr(v.w, thr);
+            }
+            *reinterpret_cast<float4 *>(tile + r * kDctTS + 4 * c4) = v;
+          }
+        } else {
+          float x[TT * kDctMC / 256];
+#pragma unroll
+          for (int u = 0; u < TT * kDctMC / 256; u++) {
+            const int i = tid + 256 * u;
+            const int r = i / kDctMC, col = i - r * kDctMC;
+            x[u] = (r < nt && col < mw) ? __ldg(src + (long long)r * a.n_mels + mc + col) : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < TT * kDctMC / 256; u++) {
+            const int i = tid + 256 * u;
+            const int r = i / kDctMC, col = i - r * kDctMC;
+            float v = x[u];
+            if (floor_on && r < nt && col < mw) v = vthr(v, thr);
+            tile[r * kDctTS + col] = v;
+          }
         }
         for (int i = tid; i < 4 * KQ * kDctMC; i += 256) {
           const int k = i / kDctMC, col = i - k * kDctMC;

@@ -164,6 +164,7 @@ def baseline_leg(plan, clips, world, args):
 def run_ours(args, rank, world, local_rank):
     import torch
     import metalmom_b200 as M
+    from metalmom_b200.shard import max_over_ranks
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -218,10 +219,7 @@ def run_ours(args, rank, world, local_rank):
     stage = np.array([plan.stage_ms(i) for i in range(min(K, 64))])
     frame_ms = float(stage[:, 1].mean())
     dct_ms = float(stage[:, 2].mean())
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, device="cuda")
     ms_step = ms / K
     value = hours_per_step * world / (ms_step / 1e3)
 
@@ -238,10 +236,7 @@ def run_ours(args, rank, world, local_rank):
     e_end.record(stream)
     torch.cuda.synchronize()
     e_ms = e_start.elapsed_time(e_end)
-    if dist is not None:
-        t = torch.tensor([e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
+    e_ms = max_over_ranks(e_ms, dist, device="cuda")
     e2e_value = hours_per_step * world / (e_ms / ke / 1e3)
     h2d = sum(c.nbytes for c in in_np)
     d2h = sum(o.nbytes for o in out_np)

@@ -175,6 +175,27 @@ MM_API int32_t mm_autotune(mm_context ctx, const MMFrontEndParams* params, int64
 MM_API int32_t mm_tune_set(int32_t n_fft, int32_t variant);
 MM_API int32_t mm_tune_get(int32_t n_fft);
 
+/* MFCC of one clip that is already in device memory, allocating nothing.
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory while they run (code inside another framework's memory pool
+ * or under a hard memory budget, real-time audio threads that may not block
+ * in the allocator, plugin hosts that forbid cudaMalloc/cudaFree): they pass
+ * the signal (d_signal, 4-byte aligned, signal_length samples) and the output
+ * d_out (min(n_mfcc, n_mels) x n_frames floats, row-major, n_frames as in
+ * mm_mfcc); all scratch comes from a 16 MiB array built into the library,
+ * which every GPU that loads the library holds until exit.  Same parameters,
+ * sentinels and results as mm_mfcc.  Returns MM_ERR_INVALID_INPUT when the
+ * clip's log-mel scratch plus tables exceed that array (about 31 000 frames,
+ * 12 minutes at 22050 Hz with hop 512, for n_fft 2048 and 128 mels).  Work is enqueued on `stream` (NULL = the default stream);
+ * the call waits once for the filterbank size, so d_out is ready after the
+ * stream synchronises.  The first call on each device looks up the array's
+ * device address, so make that first call before any stream capture.  Calls
+ * share the array: calls whose work overlaps on the GPU race. */
+MM_API int32_t mm_mfcc_noalloc(const float* d_signal, int64_t signal_length, int32_t sample_rate,
+                               int32_t n_mfcc, int32_t n_fft, int32_t hop_length, int32_t win_length,
+                               int32_t n_mels, float f_min, float f_max, int32_t center, float* d_out,
+                               void* stream);
+
 #ifdef __cplusplus
 }
 #endif

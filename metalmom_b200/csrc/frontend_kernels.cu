@@ -889,6 +889,75 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
   return cudaGetLastError();
 }
 
+// Bump allocator over caller-provided device memory (256-byte aligned pieces).
+namespace {
+struct Carver {
+  char *base;
+  size_t cap, off;
+  template <typename T>
+  T *take(size_t count) {
+    const size_t start = (off + 255) & ~size_t(255);
+    const size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+    if (start + bytes > cap) return nullptr;
+    off = start + bytes;
+    return reinterpret_cast<T *>(base + start);
+  }
+};
+}  // namespace
+
+cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, int sr, int n_fft,
+                            int win, int n_mels, float fmin, float fmax, int n_mfcc_eff, int window_zero,
+                            cudaStream_t s) {
+  const int nfreq = n_fft / 2 + 1;
+  int log2n = 0;
+  while ((1 << log2n) < n_fft) log2n++;
+  Carver c{base, cap, 0};
+  t = DevTables();
+  t.n_fft = n_fft;
+  t.n_mels = n_mels;
+  t.n_mfcc = n_mfcc_eff;
+  if (!(t.window = c.take<float>(n_fft))) return cudaErrorMemoryAllocation;
+  build_window_kernel<<<blocks_for(n_fft, 256), 256, 0, s>>>(t.window, n_fft, win, window_zero);
+  if (log2n >= 5) {
+    const int log2m = log2n - 1;
+    if (!(t.tw_stage = c.take<float2>(tw_count(log2m)))) return cudaErrorMemoryAllocation;
+    for (int q = 1; q < n_stages(log2m); q++) {
+      const int R = stage_radix(log2m, q), Ns = stage_ns(log2m, q);
+      build_stage_tw_kernel<<<blocks_for((long long)(R - 1) * Ns, 256), 256, 0, s>>>(
+          t.tw_stage + stage_tw_off(log2m, q), R, Ns);
+    }
+    if (!(t.tw_split = c.take<float2>(n_fft / 4))) return cudaErrorMemoryAllocation;
+    build_roots_kernel<<<blocks_for(n_fft / 4, 256), 256, 0, s>>>(t.tw_split, n_fft / 4, n_fft);
+  } else {
+    if (!(t.tw_tiny = c.take<float2>(n_fft))) return cudaErrorMemoryAllocation;
+    build_roots_kernel<<<1, 32, 0, s>>>(t.tw_tiny, n_fft, n_fft);
+  }
+  if (n_mels > 0) {
+    const long long cnt = (long long)n_mels * nfreq;
+    int *d_nnz = nullptr;
+    if (!(t.mel_w = c.take<float>(cnt)) || !(t.mel_info = c.take<int4>(n_mels)) || !(d_nnz = c.take<int>(1)))
+      return cudaErrorMemoryAllocation;
+    build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
+                                                          (double)fmax);
+    build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
+    mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
+    int nnz = 0;
+    cudaError_t e = cudaMemcpyAsync(&nnz, d_nnz, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    t.mel_nnz = nnz;
+    if (!(t.mel_pw = c.take<float>(nnz))) return cudaErrorMemoryAllocation;
+    mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
+  }
+  if (n_mfcc_eff > 0 && n_mels > 0) {
+    if (!(t.dct = c.take<float>((long long)n_mfcc_eff * n_mels))) return cudaErrorMemoryAllocation;
+    build_dct_kernel<<<blocks_for((long long)n_mfcc_eff * n_mels, 256), 256, 0, s>>>(t.dct, n_mfcc_eff,
+                                                                                      n_mels);
+  }
+  if (used) *used = (c.off + 255) & ~size_t(255);
+  return cudaGetLastError();
+}
+
 static int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);

@@ -84,6 +84,13 @@ int stage_twiddle_count(int log2n);
 cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, float fmin,
                          float fmax, int n_mfcc_eff, int window_zero, cudaStream_t s);
 
+// The same tables placed in caller-provided device memory [base, base+cap)
+// (no allocation); cudaErrorMemoryAllocation when they do not fit, *used =
+// bytes taken (256-byte aligned).
+cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, int sr, int n_fft,
+                            int win, int n_mels, float fmin, float fmax, int n_mfcc_eff, int window_zero,
+                            cudaStream_t s);
+
 // Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
 cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,
                             cudaStream_t s, int *launched_grid);

@@ -164,10 +164,12 @@ MM_API int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float* ms3);
 MM_API int32_t mm_plan_execute_host(mm_plan plan, const float* const* signals, float* const* outs,
                              void* stream);
 
-/* Autotuning of the frame kernel's launch variant (frames per CTA and
- * register budget), process-wide per n_fft.  mm_autotune times every variant
+/* Autotuning of the frame kernel's launch variant, process-wide per n_fft:
+ * variants 0-2 are the CTA-per-tile kernel with different frames per CTA and
+ * register budgets; variant 3 (MFCC path, n_fft 256..2048) is the
+ * warp-per-frame kernel.  mm_autotune times every variant
  * on n_clips synthetic clips of clip_samples samples (reps launches each),
- * writes the per-variant milliseconds to variant_ms (up to 3 entries), keeps
+ * writes the per-variant milliseconds to variant_ms (up to 4 entries), keeps
  * the fastest and returns it in *best_variant.  Plans and calls made
  * afterwards use the tuned variant. */
 MM_API int32_t mm_autotune(mm_context ctx, const MMFrontEndParams* params, int64_t clip_samples,

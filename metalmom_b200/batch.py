@@ -36,7 +36,7 @@ def autotune(clip_samples=661500, n_clips=32, reps=10, **params):
     synthetic clips, keep the fastest for this n_fft (process-wide) and return
     {"best": v, "ms": [per-variant ms]}."""
     p = frontend_params(**params)
-    ms = ffi.new("float[3]")
+    ms = ffi.new("float[4]")
     best = ffi.new("int32_t*")
     ctx = lib.mm_init()
     try:
@@ -45,7 +45,7 @@ def autotune(clip_samples=661500, n_clips=32, reps=10, **params):
             raise RuntimeError(f"mm_autotune failed with status {st}")
     finally:
         lib.mm_destroy(ctx)
-    n = 3 if ms[1] > 0 else 1
+    n = sum(1 for i in range(4) if ms[i] > 0)
     return {"best": int(best[0]), "ms": [float(ms[i]) for i in range(n)]}
 
 

@@ -456,7 +456,7 @@ int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *c
 }
 
 int32_t mm_tune_set(int32_t n_fft, int32_t variant) {
-  if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 || variant > 2) return MM_ERR_INVALID_INPUT;
+  if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 || variant > kWarpVariant) return MM_ERR_INVALID_INPUT;
   set_tuned_variant(ilog2(n_fft), variant);
   return MM_OK;
 }

@@ -137,6 +137,7 @@ __host__ __device__ constexpr bool tunable(int log2n, int mode, int pw) {
 }
 
 int frame_variants(int log2n, int mode, int power_is_2) {
+  if (mode == MODE_MELDB && warp_frames_per_tile(log2n) > 0) return 4;
   return tunable(log2n, mode, power_is_2 ? 0 : 1) ? 3 : 1;
 }
 
@@ -146,6 +147,7 @@ static int frames_for(int v) {
 }
 
 int frames_per_tile(int log2n, int variant) {
+  if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0) return warp_frames_per_tile(log2n);
   switch (log2n) {
     case 5: return frames_for<5>(variant);
     case 6: return frames_for<6>(variant);
@@ -725,6 +727,61 @@ __global__ void mel_offsets_kernel(int4 *info, int n_mels, int *nnz) {
   *nnz = off;
 }
 
+// Per-bin split of the dense filterbank.  A Slaney bin feeds at most two
+// consecutive bands (the falling edge of band s-1 and the rising edge of band
+// s): w2[k] = (weight of band s, weight of band s-1), bin_seg[k] = s; a bin
+// with one band m gets (weight, 0) and s = m; -1: no band; -2: a pattern the
+// split cannot express.
+__global__ void build_mel_bins_kernel(float2 *w2, int *bin_seg, const float *W, int n_mels, int nfreq) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nfreq) return;
+  int first = -1, last = -1, cnt = 0;
+  for (int m = 0; m < n_mels; m++) {
+    if (W[(long long)m * nfreq + k] != 0.0f) {  // NaN counts as nonzero
+      if (first < 0) first = m;
+      last = m;
+      cnt++;
+    }
+  }
+  if (cnt == 0) {
+    w2[k] = make_float2(0.0f, 0.0f);
+    bin_seg[k] = -1;
+  } else if (cnt == 1) {
+    w2[k] = make_float2(W[(long long)first * nfreq + k], 0.0f);
+    bin_seg[k] = first;
+  } else if (cnt == 2 && last == first + 1) {
+    w2[k] = make_float2(W[(long long)last * nfreq + k], W[(long long)first * nfreq + k]);
+    bin_seg[k] = last;
+  } else {
+    w2[k] = make_float2(0.0f, 0.0f);
+    bin_seg[k] = -2;
+  }
+}
+
+// Segment table from bin_seg (one thread): seg[s].x = first bin of segment s
+// (empty segments start where the next one does), seg[n_mels].x = one past the
+// last bin that feeds a band, seg[s].y = NaN flag of band s.  ok[1] = 1 when
+// every bin is expressible and the band of the bins never decreases.
+__global__ void build_mel_seg_kernel(int2 *seg, const int *bin_seg, const int4 *info, int n_mels, int nfreq,
+                                     int *ok) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  int prev = -1, good = 1, end = 0;
+  for (int s = 0; s <= n_mels; s++) seg[s] = make_int2(-1, s < n_mels ? info[s].w : 0);
+  for (int k = 0; k < nfreq; k++) {
+    const int s = bin_seg[k];
+    if (s == -2) good = 0;
+    if (s < 0) continue;
+    if (s < prev) good = 0;
+    if (seg[s].x < 0) seg[s].x = k;
+    end = k + 1;
+    prev = s;
+  }
+  seg[n_mels].x = end;
+  for (int s = n_mels - 1; s >= 0; s--)
+    if (seg[s].x < 0) seg[s].x = seg[s + 1].x;
+  ok[1] = good;
+}
+
 __global__ void mel_pack_kernel(float *packed, const float *W, const int4 *info, int n_mels, int nfreq) {
   const int m = blockIdx.x;
   if (m >= n_mels) return;
@@ -782,17 +839,26 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
     int *d_nnz = nullptr;
     MM_TRY(cudaMalloc(&t.mel_w, sizeof(float) * (size_t)cnt));
     MM_TRY(cudaMalloc(&t.mel_info, sizeof(int4) * (size_t)n_mels));
-    MM_TRY(cudaMalloc(&d_nnz, sizeof(int)));
+    int *bin_seg = nullptr;
+    MM_TRY(cudaMalloc(&d_nnz, 2 * sizeof(int)));
+    MM_TRY(cudaMalloc(&t.mel_w2, sizeof(float2) * (size_t)nfreq));
+    MM_TRY(cudaMalloc(&t.mel_seg, sizeof(int2) * (size_t)(n_mels + 1)));
+    MM_TRY(cudaMalloc(&bin_seg, sizeof(int) * (size_t)nfreq));
     build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
                                                           (double)fmax);
     build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
     mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
-    int nnz = 0;
-    e = cudaMemcpyAsync(&nnz, d_nnz, sizeof(int), cudaMemcpyDeviceToHost, s);
+    build_mel_bins_kernel<<<blocks_for(nfreq, 128), 128, 0, s>>>(t.mel_w2, bin_seg, t.mel_w, n_mels, nfreq);
+    build_mel_seg_kernel<<<1, 1, 0, s>>>(t.mel_seg, bin_seg, t.mel_info, n_mels, nfreq, d_nnz);
+    int nnz_ok[2] = {0, 0};
+    e = cudaMemcpyAsync(nnz_ok, d_nnz, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(d_nnz);
+    cudaFree(bin_seg);
     if (e != cudaSuccess) return e;
+    const int nnz = nnz_ok[0];
     t.mel_nnz = nnz;
+    t.mel_seg_ok = nnz_ok[1];
     MM_TRY(cudaMalloc(&t.mel_pw, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)));
     mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
   }
@@ -851,17 +917,24 @@ cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, 
   if (n_mels > 0) {
     const long long cnt = (long long)n_mels * nfreq;
     int *d_nnz = nullptr;
-    if (!(t.mel_w = c.take<float>(cnt)) || !(t.mel_info = c.take<int4>(n_mels)) || !(d_nnz = c.take<int>(1)))
+    int *bin_seg = nullptr;
+    if (!(t.mel_w = c.take<float>(cnt)) || !(t.mel_info = c.take<int4>(n_mels)) || !(d_nnz = c.take<int>(2)) ||
+        !(t.mel_w2 = c.take<float2>(nfreq)) || !(t.mel_seg = c.take<int2>(n_mels + 1)) ||
+        !(bin_seg = c.take<int>(nfreq)))
       return cudaErrorMemoryAllocation;
     build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
                                                           (double)fmax);
     build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
     mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
-    int nnz = 0;
-    cudaError_t e = cudaMemcpyAsync(&nnz, d_nnz, sizeof(int), cudaMemcpyDeviceToHost, s);
+    build_mel_bins_kernel<<<blocks_for(nfreq, 128), 128, 0, s>>>(t.mel_w2, bin_seg, t.mel_w, n_mels, nfreq);
+    build_mel_seg_kernel<<<1, 1, 0, s>>>(t.mel_seg, bin_seg, t.mel_info, n_mels, nfreq, d_nnz);
+    int nnz_ok[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(nnz_ok, d_nnz, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return e;
+    const int nnz = nnz_ok[0];
     t.mel_nnz = nnz;
+    t.mel_seg_ok = nnz_ok[1];
     if (!(t.mel_pw = c.take<float>(nnz))) return cudaErrorMemoryAllocation;
     mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
   }
@@ -964,6 +1037,8 @@ cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a
       return launch_mode<MODE_MEL, 2>(log2n, variant, a, grid_limit, s, launched);
     case MODE_MELDB:
       if (pw != 0) return cudaErrorInvalidValue;
+      if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0)
+        return launch_frontend_warp(log2n, a, grid_limit, s, launched);
       return launch_mode<MODE_MELDB, 0>(log2n, variant, a, grid_limit, s, launched);
     default: return cudaErrorInvalidValue;
   }

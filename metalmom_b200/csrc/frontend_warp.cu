@@ -1,0 +1,558 @@
+// Warp-per-frame front-end kernel (launch variant 3, n_fft 256..2048, MFCC
+// path): framing + periodic Hann + real FFT + |X|^2 + Slaney mel + log10 per
+// frame, with a running per-clip maximum for top_db.
+//
+// The reference computes the same per frame on the CPU, one frame after the
+// other (STFT.swift:287-335 window/FFT/power, MelSpectrogram.swift:122-138 mel,
+// Scaling.swift:73-118 dB).  Here a frame is owned by TPF = n_fft/64 lanes of a
+// warp; each lane holds 32 complex points of the packed sequence
+// z[n] = x[2n] w[2n] + i x[2n+1] w[2n+1] (M = n_fft/2 points):
+//
+//   n = j + TPF r   (j = lane in the frame group, r = register)
+//   k = k1 + 32 k2
+//   stage 1: 32-point DFT over r in registers       -> Y[j][k1]
+//            twiddle W_M^(j k1)
+//   one shared-memory transpose (row stride 33, conflict-free)
+//   stage 2: TPF-point DFTs over j in registers      -> Z[k1 + 32 k2]
+//   real split X[k] = E + W_N^k O, X[M-k] = conj(E - W_N^k O), both from the
+//   pair (Z[k], Z[M-k]): the stage-2 columns are dealt to lanes so that k1
+//   and 32-k1 sit in the same lane (TPF < 32); for TPF = 32 the partner lanes
+//   l and 32-l swap the upper 16 registers by shuffle and each takes 16 pairs.
+//
+// Only warp-level synchronisation is used.  The spectrum is kept as |2X|^2
+// (the 1/2 of E and O is not applied) and the mel sums are scaled by 1/4,
+// which is exact in float arithmetic.  The window, the stage-2 twiddles and
+// the mel tables are staged in shared memory once per CTA.
+#include <math.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "fft_radix.cuh"
+#include "frame_common.cuh"
+#include "kernels.h"
+
+namespace mm {
+
+// ---------------------------------------------------------------------------
+// compile-time cos / sin of 2 pi k / d: octant reduction, then Taylor series
+// in double (|x| <= pi/4, 12 terms: error far below float rounding)
+// ---------------------------------------------------------------------------
+constexpr double kPiD = 3.14159265358979323846264338327950288;
+
+__host__ __device__ constexpr double ce_sin_q(double x) {
+  double term = x, sum = x;
+  for (int n = 1; n < 12; n++) {
+    term *= -x * x / (double)((2 * n) * (2 * n + 1));
+    sum += term;
+  }
+  return sum;
+}
+__host__ __device__ constexpr double ce_cos_q(double x) {
+  double term = 1.0, sum = 1.0;
+  for (int n = 1; n < 12; n++) {
+    term *= -x * x / (double)((2 * n - 1) * (2 * n));
+    sum += term;
+  }
+  return sum;
+}
+// which = 0: cos(2 pi k / d), 1: sin(2 pi k / d)
+__host__ __device__ constexpr double ce_trig(long long k, long long d, int which) {
+  k %= d;
+  if (k < 0) k += d;
+  const long long q = (8 * k) / d;                                   // octant 0..7
+  const double phi = kPiD * (double)(8 * k - q * d) / (4.0 * (double)d);  // in [0, pi/4)
+  const double psi = kPiD * (double)(d * (q + 1) - 8 * k) / (4.0 * (double)d);  // pi/4 - phi
+  double c = 0.0, s = 0.0;
+  switch (q) {
+    case 0: c = ce_cos_q(phi); s = ce_sin_q(phi); break;
+    case 1: c = ce_sin_q(psi); s = ce_cos_q(psi); break;
+    case 2: c = -ce_sin_q(phi); s = ce_cos_q(phi); break;
+    case 3: c = -ce_cos_q(psi); s = ce_sin_q(psi); break;
+    case 4: c = -ce_cos_q(phi); s = -ce_sin_q(phi); break;
+    case 5: c = -ce_sin_q(psi); s = -ce_cos_q(psi); break;
+    case 6: c = ce_sin_q(phi); s = -ce_cos_q(phi); break;
+    default: c = ce_cos_q(psi); s = -ce_sin_q(psi); break;
+  }
+  return which == 0 ? c : s;
+}
+
+template <int I, int N, typename Fn>
+__device__ __forceinline__ void static_for(Fn &&fn) {
+  if constexpr (I < N) {
+    fn(std::integral_constant<int, I>{});
+    static_for<I + 1, N>(fn);
+  }
+}
+
+// a * exp(-2 pi i K / D), with the exact special angles spelled out.
+template <int K, int D>
+__device__ __forceinline__ cpx tw_const(cpx a) {
+  constexpr int k = ((K % D) + D) % D;
+  if constexpr (k == 0) {
+    return a;
+  } else if constexpr (4 * k == D) {
+    return mul_mi(a);
+  } else if constexpr (2 * k == D) {
+    return {-a.x, -a.y};
+  } else if constexpr (4 * k == 3 * D) {
+    return mul_pi(a);
+  } else if constexpr (8 * k == D) {
+    return mul_w8_1(a);
+  } else if constexpr (8 * k == 3 * D) {
+    return mul_w8_3(a);
+  } else if constexpr (8 * k == 5 * D) {
+    return {-kR * (a.x + a.y), kR * (a.x - a.y)};
+  } else if constexpr (8 * k == 7 * D) {
+    return {kR * (a.x - a.y), kR * (a.x + a.y)};
+  } else {
+    constexpr float c = (float)ce_trig(k, D, 0);
+    constexpr float s = -(float)ce_trig(k, D, 1);
+    return {fmaf(a.x, c, -a.y * s), fmaf(a.x, s, a.y * c)};
+  }
+}
+
+// In-place 32-point DFT, natural order: radix-2 decimation in time over two
+// 16-point DFTs.
+__device__ __forceinline__ void dft32(cpx *v) {
+  cpx e[16], o[16];
+#pragma unroll
+  for (int m = 0; m < 16; m++) {
+    e[m] = v[2 * m];
+    o[m] = v[2 * m + 1];
+  }
+  dft16(e);
+  dft16(o);
+  static_for<0, 16>([&](auto ki) {
+    constexpr int k = decltype(ki)::value;
+    const cpx t = tw_const<k, 32>(o[k]);
+    v[k] = cadd(e[k], t);
+    v[k + 16] = csub(e[k], t);
+  });
+}
+
+template <int R>
+__device__ __forceinline__ void dft_any(cpx *v) {
+  if constexpr (R == 32) dft32(v);
+  else dft<R>(v);
+}
+
+// W_N^s for any s >= 0 from the quarter table q[t] = W_N^t, t < N/4.
+__device__ __forceinline__ cpx root_q(const float2 *q, int s, int N) {
+  s &= N - 1;
+  const int quarter = N >> 2;
+  const int h = s / quarter, r = s - h * quarter;
+  const float2 w = __ldg(q + r);
+  switch (h) {
+    case 0: return {w.x, w.y};
+    case 1: return {w.y, -w.x};   // * (-i)
+    case 2: return {-w.x, -w.y};  // * (-1)
+    default: return {-w.y, w.x};  // * (+i)
+  }
+}
+
+// Samples (x[i], x[i+1]) for i = first + stride r, r < 32, with the padding
+// rule of sample_at; used only for frames that overlap the clip's edges.
+__device__ __noinline__ void gather_edge(cpx *out, const float *sig, long long first, long long length,
+                                         int pad_mode, int stride) {
+  for (int r = 0; r < 32; r++) {
+    const long long n0 = first + (long long)stride * r;
+    out[r] = {sample_at(sig, n0, length, pad_mode), sample_at(sig, n0 + 1, length, pad_mode)};
+  }
+}
+
+template <int LOG2N>
+struct WShape {
+  static constexpr int N = 1 << LOG2N;
+  static constexpr int M = N / 2;
+  static constexpr int TPF = M / 32;     // lanes per frame
+  static constexpr int FPW = 32 / TPF;   // frames per warp
+  static constexpr int C = FPW;          // stage-2 columns per lane
+  static constexpr int HALF = C / 2;
+  static constexpr int FSTRIDE = TPF * 33;  // complex slots per frame buffer
+  static constexpr int NW = 8;              // warps per CTA
+  static constexpr int THREADS = 32 * NW;
+  static constexpr int F = NW * FPW;        // frames per CTA tile
+  static_assert(TPF >= 4 && TPF <= 32, "n_fft must be 256..2048");
+};
+
+template <int LOG2N>
+__host__ __device__ constexpr size_t warp_fixed_smem() {
+  using S = WShape<LOG2N>;
+  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + size_t(S::F) * S::FSTRIDE * 8;
+}
+
+int warp_frames_per_tile(int log2n) {
+  switch (log2n) {
+    case 8: return WShape<8>::F;
+    case 9: return WShape<9>::F;
+    case 10: return WShape<10>::F;
+    case 11: return WShape<11>::F;
+    default: return 0;
+  }
+}
+
+// stage-2 column of slot c for lane l (see the header comment)
+template <int TPF, int C, int c>
+__device__ __forceinline__ int stage2_col(int l) {
+  if constexpr (C == 1) {
+    return l;
+  } else if constexpr (c < C / 2) {
+    return l + TPF * c;
+  } else if constexpr (c == C / 2) {
+    return l == 0 ? 16 : 32 - l;
+  } else {
+    return 32 - l - TPF * (c - C / 2);
+  }
+}
+
+template <int LOG2N>
+__global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(FrontArgs a) {
+  using S = WShape<LOG2N>;
+  constexpr int N = S::N, M = S::M, TPF = S::TPF, C = S::C, HALF = S::HALF, F = S::F;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nmel = a.n_mels;
+  // Per-bin split of the filterbank (else packed rows).
+  const bool split = a.mel_seg_ok != 0;
+  const bool mel_in_smem = a.mel_nnz <= kMelSmemMax;
+  unsigned char *sp = smem;
+  cpx *tw2 = reinterpret_cast<cpx *>(sp);  // W_M^(j k1), [k1-1][j]
+  sp += align16(size_t(31) * TPF * 8);
+  float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
+  sp += align16(size_t(N) * 4);
+  cpx *bufs = reinterpret_cast<cpx *>(sp);
+  sp += size_t(F) * S::FSTRIDE * 8;
+  int4 *mel_s = reinterpret_cast<int4 *>(sp);  // packed rows: mel_info
+  int2 *seg_s = reinterpret_cast<int2 *>(sp);  // split: mel_seg (n_mels + 1 entries)
+  sp += 16 * (size_t)(nmel + 1);
+  float2 *w2_s = reinterpret_cast<float2 *>(sp);  // split: per-bin weights, M + 1 entries
+  float *melw_s = reinterpret_cast<float *>(sp);  // packed rows
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int grp = lane / TPF;       // frame of this lane within the warp
+  const int l = lane - grp * TPF;   // lane within the frame group
+  const float2 *twq = a.tw_split;   // W_N^t, t < N/4
+
+  for (int i = tid; i < 31 * TPF; i += S::THREADS) {
+    const int k1 = i / TPF + 1, j = i - (k1 - 1) * TPF;
+    tw2[i] = root_q(twq, 2 * j * k1, N);
+  }
+  for (int i = tid; i < N / 4; i += S::THREADS)
+    reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+  if (split) {
+    for (int i = tid; i <= nmel; i += S::THREADS) seg_s[i] = __ldg(a.mel_seg + i);
+    for (int i = tid; i <= M; i += S::THREADS) w2_s[i] = __ldg(a.mel_w2 + i);
+  } else {
+    for (int i = tid; i < nmel; i += S::THREADS) mel_s[i] = __ldg(a.mel_info + i);
+    if (mel_in_smem)
+      for (int i = tid; i < a.mel_nnz; i += S::THREADS) melw_s[i] = __ldg(a.mel_pw + i);
+  }
+  const float *melw = mel_in_smem ? melw_s : a.mel_pw;
+  __syncthreads();
+
+  // real-split bases W_N^(first bin of each column pair)
+  cpx base_c[HALF > 0 ? HALF : 1];
+  cpx base_hi;
+  if constexpr (C == 1) {
+    base_c[0] = root_q(twq, l, N);
+    base_hi = base_c[0];
+  } else {
+#pragma unroll
+    for (int c = 0; c < HALF; c++) base_c[c] = root_q(twq, l + TPF * c, N);
+    base_hi = (l == 0) ? root_q(twq, 16 + 3 * (N / 4), N) : base_c[0];
+  }
+
+  cpx *fb = bufs + (warp * S::FPW + grp) * S::FSTRIDE;
+  float *P = reinterpret_cast<float *>(fb);
+  const unsigned gmask = (TPF == 32) ? FULL : (((1u << TPF) - 1u) << (grp * TPF));
+
+  const int total = a.total_tiles;
+  const int t_begin = (int)((long long)blockIdx.x * total / gridDim.x);
+  const int t_end = (int)((long long)(blockIdx.x + 1) * total / gridDim.x);
+  int cur = -1;
+  float vmax = -INFINITY;
+
+  for (int tile = t_begin; tile < t_end; tile++) {
+    const int c = __ldg(a.tile_clip + tile);
+    if (c != cur) {  // warp-uniform: every frame of a tile belongs to one clip
+      float m = vmax;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+      if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+      cur = c;
+      vmax = -INFINITY;
+    }
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int t = (tile - cd.tile_base) * F + warp * S::FPW + grp;
+    if constexpr (TPF == 32) {
+      if (t >= cd.n_frames) continue;  // warp-uniform
+    }
+    const bool valid = t < cd.n_frames;
+    const long long s0 = (long long)t * a.hop - a.pad;
+    const float *sig = a.signal + cd.sig_off;
+
+    // ---- gather: v[r] = (x[2n], x[2n+1]) for n = l + TPF r
+    cpx v[32];
+    if (s0 >= 0 && s0 + N <= cd.length) {
+      const float *base = sig + s0 + 2 * l;
+      if (((cd.sig_off + s0) & 1) == 0) {
+#pragma unroll
+        for (int r = 0; r < 32; r++) {
+          const float2 x = __ldg(reinterpret_cast<const float2 *>(base + 2 * TPF * r));
+          v[r] = {x.x, x.y};
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 32; r++) v[r] = {__ldg(base + 2 * TPF * r), __ldg(base + 2 * TPF * r + 1)};
+      }
+    } else {
+      // frames that reach into the padding (a few per clip): out of line, so
+      // that their index arithmetic does not weigh on the interior path
+      cpx tmp[32];
+      gather_edge(tmp, sig, s0 + 2 * l, cd.length, a.pad_mode, 2 * TPF);
+#pragma unroll
+      for (int r = 0; r < 32; r++) v[r] = tmp[r];
+    }
+    // ---- window
+    {
+      const float2 *wb = reinterpret_cast<const float2 *>(win_s) + l;
+#pragma unroll
+      for (int r = 0; r < 32; r++) {
+        const float2 w = wb[TPF * r];
+        v[r].x *= w.x;
+        v[r].y *= w.y;
+      }
+    }
+
+    // ---- stage 1: 32-point DFT over registers; its last butterflies are
+    // followed directly by the twiddle W_M^(l k1) and the store into row l of
+    // the frame buffer (stride 33), so that registers free up as it goes.
+    __syncwarp();  // the previous frame's mel reads of P are done
+    {
+      cpx e[16], o[16];
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        e[m] = v[2 * m];
+        o[m] = v[2 * m + 1];
+      }
+      dft16(e);
+      dft16(o);
+      cpx *row = fb + l * 33;
+      static_for<0, 16>([&](auto ki) {
+        constexpr int k = decltype(ki)::value;
+        const cpx t = tw_const<k, 32>(o[k]);
+        cpx lo = cadd(e[k], t), hi = csub(e[k], t);
+        if constexpr (k > 0) lo = cmul(lo, tw2[(k - 1) * TPF + l]);
+        hi = cmul(hi, tw2[(k + 15) * TPF + l]);
+        row[k] = lo;
+        row[k + 16] = hi;
+      });
+    }
+    __syncwarp();
+    static_for<0, C>([&](auto ci) {
+      constexpr int cc = decltype(ci)::value;
+      const int col = stage2_col<TPF, C, cc>(l);
+#pragma unroll
+      for (int jj = 0; jj < TPF; jj++) v[cc * TPF + jj] = fb[jj * 33 + col];
+    });
+    // ---- stage 2: TPF-point DFTs, v[c*TPF + k2] = Z[col(c) + 32 k2]
+#pragma unroll
+    for (int cc = 0; cc < C; cc++) dft_any<TPF>(v + cc * TPF);
+    __syncwarp();  // every lane has read its columns: fb becomes P
+
+    // ---- real split, P[k] = |2 X[k]|^2
+    float chk = 0.0f;
+    if constexpr (C == 1) {
+      // lanes l and 32-l swap registers 16..31: pair i of lane l is
+      // (Z[l + 32 i], Z[M - l - 32 i]) = (v[i], partner's v[31 - i]); lane 0
+      // pairs with itself: (v[i], v[32 - i]) and the self pair v[16] (k = M/2).
+      const int src = (32 - l) & 31;
+      cpx rcv[16];
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        rcv[m].x = __shfl_sync(FULL, v[16 + m].x, src);
+        rcv[m].y = __shfl_sync(FULL, v[16 + m].y, src);
+      }
+      const bool l0 = (l == 0);
+      static_for<0, 16>([&](auto ki) {
+        constexpr int i = decltype(ki)::value;
+        const cpx za = v[i];
+        cpx zb;
+        if constexpr (i == 0) zb = l0 ? v[0] : rcv[15];
+        else zb = l0 ? rcv[16 - i] : rcv[15 - i];
+        const float ex = za.x + zb.x, ey = za.y - zb.y;
+        const float ox = za.y + zb.y, oy = zb.x - za.x;
+        const cpx w = tw_const<i, 64>(base_c[0]);
+        const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
+        const float xr = ex + wr, xi = ey + wi;
+        const float yr = ex - wr, yi = ey - wi;
+        const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr, yr, yi * yi);
+        const int ka = l + 32 * i;
+        P[ka] = p;
+        P[M - ka] = q;
+        chk += p + q;
+      });
+      if (l0) {
+        const float p = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
+        P[M / 2] = p;
+        chk += p;
+      }
+    } else {
+      const bool l0 = (l == 0);
+      static_for<0, HALF>([&](auto ci) {
+        constexpr int cc = decltype(ci)::value;
+        static_for<0, TPF>([&](auto ki) {
+          constexpr int k2 = decltype(ki)::value;
+          cpx za, zb, base;
+          int ka;
+          if constexpr (cc == 0) {
+            constexpr bool lo = k2 < TPF / 2;
+            constexpr int ia0 = lo ? k2 : HALF * TPF + (k2 - TPF / 2);
+            constexpr int ib0 = lo ? (TPF - k2) % TPF : HALF * TPF + TPF - 1 - (k2 - TPF / 2);
+            constexpr int ia = k2, ib = HALF * TPF + TPF - 1 - k2;
+            za = l0 ? v[ia0] : v[ia];
+            zb = l0 ? v[ib0] : v[ib];
+            base = lo ? base_c[0] : base_hi;
+            ka = l0 ? (lo ? 32 * k2 : 16 + 32 * (k2 - TPF / 2)) : l + 32 * k2;
+          } else {
+            za = v[cc * TPF + k2];
+            zb = v[(cc + HALF) * TPF + TPF - 1 - k2];
+            base = base_c[cc];
+            ka = l + TPF * cc + 32 * k2;
+          }
+          const float ex = za.x + zb.x, ey = za.y - zb.y;
+          const float ox = za.y + zb.y, oy = zb.x - za.x;
+          const cpx w = tw_const<k2, 2 * TPF>(base);
+          const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
+          const float xr = ex + wr, xi = ey + wi;
+          const float yr = ex - wr, yi = ey - wi;
+          const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr, yr, yi * yi);
+          P[ka] = p;
+          P[M - ka] = q;
+          chk += p + q;
+        });
+      });
+      if (l0) {
+        const cpx zm = v[TPF / 2];
+        const float p = 4.0f * fmaf(zm.x, zm.x, zm.y * zm.y);
+        P[M / 2] = p;
+        chk += p;
+      }
+    }
+    const bool bad = (__ballot_sync(FULL, !isfinite(chk)) & gmask) != 0;
+    __syncwarp();  // P complete
+
+    // ---- log-mel row of this frame + running clip max
+    float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
+    if (split) {
+      // band m = R[m] + F[m+1]: lane l sums segment s = it*TPF + l (each bin
+      // read once, two products); F[s+1] comes from the next lane, or for the
+      // group's last lane from lane 0 of the following pass (passes run from
+      // the top band down).
+      const int passes = (nmel + TPF - 1) / TPF;
+      float carry = 0.0f;
+      for (int it = passes - 1; it >= 0; it--) {
+        const int sg = it * TPF + l;
+        float R0 = 0.0f, F0 = 0.0f, R1 = 0.0f, F1 = 0.0f;
+        int nanrow = 0;
+        if (sg < nmel) {
+          const int2 g0 = seg_s[sg];
+          const int k0 = g0.x, k1 = seg_s[sg + 1].x;
+          int k = k0;
+          for (; k + 1 < k1; k += 2) {
+            const float2 wa = w2_s[k], wb = w2_s[k + 1];
+            const float pa = P[k], pb = P[k + 1];
+            R0 = fmaf(wa.x, pa, R0);
+            F0 = fmaf(wa.y, pa, F0);
+            R1 = fmaf(wb.x, pb, R1);
+            F1 = fmaf(wb.y, pb, F1);
+          }
+          if (k < k1) {
+            const float2 wa = w2_s[k];
+            const float pa = P[k];
+            R0 = fmaf(wa.x, pa, R0);
+            F0 = fmaf(wa.y, pa, F0);
+          }
+          nanrow = g0.y;
+        }
+        const float R = R0 + R1, F = F0 + F1;
+        float Fn = __shfl_down_sync(FULL, F, 1, TPF);
+        const float Ffirst = __shfl_sync(FULL, F, 0, TPF);
+        if (l == TPF - 1) Fn = carry;
+        carry = Ffirst;
+        if (sg < nmel) {
+          float acc = 0.25f * (R + Fn);
+          if (nanrow || bad) acc = __int_as_float(0x7fc00000);
+          const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+          if (valid) {
+            dst[sg] = val;
+            vmax = fmaxf(vmax, val);
+          }
+        }
+      }
+    } else {
+      for (int m = l; m < nmel; m += TPF) {
+        const float acc = 0.25f * mel_dot(mel_s[m], melw, P, bad);
+        const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        if (valid) {
+          dst[m] = val;
+          vmax = fmaxf(vmax, val);
+        }
+      }
+    }
+  }
+  float m = vmax;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+  if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+}
+
+static int sm_count_w() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int LOG2N>
+static cudaError_t launch_warp_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  using S = WShape<LOG2N>;
+  const size_t split_bytes = align16(8 * (size_t)(S::M + 1));
+  const size_t smem = warp_fixed_smem<LOG2N>() + 16 * (size_t)(a.n_mels + 1) +
+                      std::max(split_bytes, mel_smem_bytes(0, a.mel_nnz));
+  static size_t configured = 0;
+  auto kern = frame_warp_kernel<LOG2N>;
+  cudaError_t e;
+  if (smem > 48 * 1024 && smem > configured) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = smem;
+  }
+  int per_sm = 1;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, S::THREADS, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  long long grid = (long long)sm_count_w() * per_sm;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  if (grid < 1) return cudaSuccess;
+  kern<<<(unsigned)grid, S::THREADS, smem, s>>>(a);
+  if (launched) *launched = (int)grid;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,
+                                 int *launched) {
+  if (launched) *launched = 0;
+  if (a.total_tiles <= 0) return cudaSuccess;
+  switch (log2n) {
+    case 8: return launch_warp_t<8>(a, grid_limit, s, launched);
+    case 9: return launch_warp_t<9>(a, grid_limit, s, launched);
+    case 10: return launch_warp_t<10>(a, grid_limit, s, launched);
+    case 11: return launch_warp_t<11>(a, grid_limit, s, launched);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace mm

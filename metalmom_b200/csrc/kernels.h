@@ -35,6 +35,13 @@ struct DevTables {
   float *mel_pw = nullptr;     // packed nonzero weights, row after row
   int4 *mel_info = nullptr;    // per mel {start bin, count, packed offset, nan-row flag}
   int mel_nnz = 0;             // entries of mel_pw
+  // Per-bin split of the same filterbank (warp kernel): bin k feeds band s(k)
+  // with mel_w2[k].x and band s(k)-1 with mel_w2[k].y.  Segment s = the bins
+  // [mel_seg[s].x, mel_seg[s+1].x) (n_mels + 1 entries; .y = NaN-row flag of
+  // band s).
+  float2 *mel_w2 = nullptr;
+  int2 *mel_seg = nullptr;
+  int mel_seg_ok = 0;          // 0: the split does not describe the filterbank (use mel_pw)
   float *dct = nullptr;        // [n_mfcc_eff][n_mels] DCT-II ortho basis
 };
 
@@ -51,6 +58,9 @@ struct FrontArgs {
   const int4 *mel_info;
   const float *mel_pw;  // packed weights (mel_info[m].z = offset of row m)
   int mel_nnz;
+  const float2 *mel_w2;  // per-bin split (see DevTables)
+  const int2 *mel_seg;
+  int mel_seg_ok;
   int n_mels;
   float power;  // exponent applied to |X| (2 = power spectrum)
   float amin, ref;
@@ -77,6 +87,11 @@ constexpr int kDctTile = 64;  // frames per DCT tile
 int frames_per_tile(int log2n, int variant);
 // Number of launch variants the autotuner may choose from (1 = not tunable).
 int frame_variants(int log2n, int mode, int power_is_2);
+// Launch variant 3: the warp-per-frame kernel (MODE_MELDB, n_fft 256..2048).
+constexpr int kWarpVariant = 3;
+int warp_frames_per_tile(int log2n);  // 0 when the size has no warp kernel
+cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,
+                                 int *launched);
 // Stockham twiddle table length (entries) for log2(n_fft) >= 5.
 int stage_twiddle_count(int log2n);
 

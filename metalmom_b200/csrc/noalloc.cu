@@ -169,6 +169,9 @@ extern "C" MM_API int32_t mm_mfcc_noalloc(const float *d_signal, int64_t signal_
   a.mel_info = t.mel_info;
   a.mel_pw = t.mel_pw;
   a.mel_nnz = t.mel_nnz;
+  a.mel_w2 = t.mel_w2;
+  a.mel_seg = t.mel_seg;
+  a.mel_seg_ok = t.mel_seg_ok;
   a.n_mels = g.n_mels;
   a.power = 2.0f;
   a.amin = g.amin;

@@ -118,6 +118,8 @@ const DevTables *get_tables(const Group &g, int *status) {
     cudaFree(t->mel_w);
     cudaFree(t->mel_pw);
     cudaFree(t->mel_info);
+    cudaFree(t->mel_w2);
+    cudaFree(t->mel_seg);
     cudaFree(t->dct);
     delete t;
     return nullptr;
@@ -252,6 +254,9 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.mel_info = t->mel_info;
   a.mel_pw = t->mel_pw;
   a.mel_nnz = t->mel_nnz;
+  a.mel_w2 = t->mel_w2;
+  a.mel_seg = t->mel_seg;
+  a.mel_seg_ok = t->mel_seg_ok;
   a.n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
   a.power = g.power;
   a.amin = g.amin;

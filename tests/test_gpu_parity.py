@@ -283,7 +283,7 @@ def test_every_launch_variant_vs_oracle(n_fft):
     exp_mel = O.melspectrogram(y, SR, n_fft, n_fft // 4, n_fft, True, 2.0, 64)
     old = M.tune_get(n_fft)
     try:
-        for v in range(3):
+        for v in range(4):
             M.tune_set(n_fft, v)
             got = M.mfcc(y, sr=SR, n_fft=n_fft, hop_length=n_fft // 4, n_mels=64)
             assert O.mfcc_rel_error(got, exp) < MFCC_TOL, (v, O.mfcc_rel_error(got, exp))
@@ -293,9 +293,46 @@ def test_every_launch_variant_vs_oracle(n_fft):
         M.tune_set(n_fft, old)
 
 
+@pytest.mark.parametrize("n_fft,win,hop,pad_mode", [
+    (2048, 2048, 512, "constant"),
+    (2048, 2048, 441, "reflect"),   # odd hop: frame starts alternate between even and odd samples
+    (1024, 1024, 256, "constant"),
+    (512, 400, 160, "constant"),    # window shorter than n_fft
+    (512, 512, 128, "reflect"),
+    (256, 256, 64, "constant"),
+])
+def test_warp_kernel_uneven_batch_vs_oracle(n_fft, win, hop, pad_mode):
+    """Variant 3 (one warp per frame) on uneven clips: clips shorter than a
+    frame, clips whose start is not 8-byte aligned in the batch buffer, and
+    frames that reach into the padding on both ends."""
+    rng = np.random.default_rng(n_fft + hop)
+    lens = [1, 3, n_fft // 2 + 1, n_fft - 1, n_fft + 1, 5 * n_fft + 3] + \
+           [int(x) for x in rng.integers(1000, 60000, 5)]
+    if pad_mode == "reflect":
+        lens = [L for L in lens if L > n_fft // 2]  # reflect needs L > n_fft/2
+    clips = [synth.music_clip(L, SR, seed=1000 + i) for i, L in enumerate(lens)]
+    old = M.tune_get(n_fft)
+    try:
+        M.tune_set(n_fft, 3)
+        outs = M.mfcc_batch(clips, sr=SR, n_fft=n_fft, hop_length=hop, win_length=win, n_mels=64,
+                            pad_mode=pad_mode)
+        single = M.mfcc(clips[-1], sr=SR, n_fft=n_fft, hop_length=hop, win_length=win, n_mels=64) \
+            if pad_mode == "constant" else None
+    finally:
+        M.tune_set(n_fft, old)
+    pm = O.PAD_REFLECT if pad_mode == "reflect" else O.PAD_CONSTANT
+    for c, o in zip(clips, outs):
+        exp = O.mfcc(c, SR, 20, n_fft, hop, win, 64, pad_mode=pm)
+        assert o.shape == exp.shape
+        if exp.size:
+            assert O.mfcc_rel_error(o, exp) < MFCC_TOL, (len(c), O.mfcc_rel_error(o, exp))
+    if single is not None:
+        np.testing.assert_array_equal(single, outs[-1])
+
+
 def test_autotune_picks_a_variant_and_keeps_parity():
     res = M.autotune(clip_samples=22050 * 5, n_clips=8, reps=3, sr=SR, n_fft=2048, hop_length=512)
-    assert res["best"] in (0, 1, 2) and len(res["ms"]) == 3 and all(m > 0 for m in res["ms"])
+    assert res["best"] in (0, 1, 2, 3) and len(res["ms"]) == 4 and all(m > 0 for m in res["ms"])
     assert M.tune_get(2048) == res["best"]
     y = synth.music_clip(22050 * 4, SR, seed=9)
     got = M.mfcc(y, sr=SR)

@@ -177,6 +177,53 @@ MM_API int32_t mm_autotune(mm_context ctx, const MMFrontEndParams* params, int64
 MM_API int32_t mm_tune_set(int32_t n_fft, int32_t variant);
 MM_API int32_t mm_tune_get(int32_t n_fft);
 
+/* ---- Serving: continuous batching with device-memory admission --------- */
+
+/* Returned by mm_server_poll / mm_server_wait while a request is not done. */
+#define MM_PENDING 1
+
+/* A server owns a scheduler thread and max_inflight CUDA streams.  Requests
+ * (one clip + its MFCC parameters each) are queued by mm_server_submit; the
+ * scheduler groups pending requests by parameter set into batches (oldest
+ * first, up to max_batch_clips and the free part of device_budget_bytes) and
+ * starts a batch whenever a stream is free, so requests that arrive while
+ * others run are admitted as streams and memory free up, and batches of
+ * different groups overlap on the device.  Tables stay resident per group.
+ * Results are identical to mm_mfcc_batch on the same clip.  All calls are
+ * thread-safe; no call may be in progress while mm_server_destroy runs. */
+typedef void* mm_server;
+
+typedef struct {
+    int64_t device_budget_bytes; /* device memory of the batches in flight; <= 0: 40 GiB */
+    int32_t max_batch_clips;     /* <= 0: 256 */
+    int32_t max_inflight;        /* batches on the device at once; <= 0: 4 (at most 64) */
+} MMServerConfig;
+
+typedef struct {
+    int64_t submitted, completed, failed, pending, inflight_batches, batches_launched;
+    int64_t bytes_in_use, peak_bytes_in_use;
+    double audio_seconds_completed;
+    double latency_p50_ms, latency_p99_ms, latency_mean_ms, latency_max_ms; /* submit -> result */
+} MMServerStats;
+
+MM_API mm_server mm_server_create(const MMServerConfig* config, int32_t* status);
+/* Finishes the batches in flight, drops requests that never started and
+ * frees every undelivered result. */
+MM_API void mm_server_destroy(mm_server server);
+/* Copies the samples; *request_id identifies the request.  A request with no
+ * frame or no coefficient is rejected (MM_ERR_INVALID_INPUT); a request
+ * whose batch alone exceeds the budget fails with MM_ERR_ALLOC_FAILED. */
+MM_API int32_t mm_server_submit(mm_server server, const float* signal, int64_t length,
+                                const MMFrontEndParams* params, int64_t* request_id);
+/* MM_PENDING while running; otherwise moves the result ([rows, n_frames],
+ * free with mm_buffer_free) into *out, or returns the request's error, and
+ * forgets the request. */
+MM_API int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer* out);
+/* As mm_server_poll, waiting up to timeout_ms (< 0: no limit). */
+MM_API int32_t mm_server_wait(mm_server server, int64_t request_id, int32_t timeout_ms, MMBuffer* out);
+MM_API int32_t mm_server_stats(mm_server server, MMServerStats* out);
+MM_API int32_t mm_server_reset_stats(mm_server server);
+
 /* MFCC of one clip that is already in device memory, allocating nothing.
  * No counterpart in the reference.  For callers that must not allocate
  * device memory while they run (code inside another framework's memory pool

@@ -3,12 +3,14 @@
 ``stft``, ``melspectrogram``, ``mfcc``, ``power_to_db`` and ``amplitude_to_db``
 keep the names, defaults and error behaviour of MetalMom's Python package and
 run on the GPU through ``libmetalmom.so``; ``mfcc_batch`` and ``Plan`` add a
-batched, device-resident path.
+batched, device-resident path and ``Server`` a continuously batching request
+loop.
 """
 
 from .core import stft
 from .feature import amplitude_to_db, melspectrogram, mfcc, power_to_db
 from .batch import Plan, autotune, frontend_params, mfcc_batch, tune_get, tune_set
+from .serve import Server
 
 __all__ = ["stft", "melspectrogram", "mfcc", "power_to_db", "amplitude_to_db",
-           "mfcc_batch", "Plan", "frontend_params", "autotune", "tune_get", "tune_set"]
+           "mfcc_batch", "Plan", "frontend_params", "autotune", "tune_get", "tune_set", "Server"]

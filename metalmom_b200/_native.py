@@ -58,6 +58,6 @@ ffi.cdef(header_cdef())
 if not os.path.exists(LIB_PATH):
     raise RuntimeError(
         f"libmetalmom.so not found at {LIB_PATH}. "
-        "Build it with `python -m metalmom_b200.build`.")
+        "Build it with `python metalmom_b200/build.py`.")
 
 lib = ffi.dlopen(LIB_PATH)

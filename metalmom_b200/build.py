@@ -1,6 +1,8 @@
 """Build libmetalmom.so (CUDA kernels + C ABI) for sm_100a, in tree.
 
-    python -m metalmom_b200.build          # or python metalmom_b200/build.py
+    python metalmom_b200/build.py [--force]
+
+(run as a script: importing the package itself needs the built library).
 
 Sources: metalmom_b200/csrc/*.cu; output: metalmom_b200/_lib/libmetalmom.so.
 The CUDA runtime is linked statically, so the library needs only the driver.
@@ -17,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libmetalmom.so")
-SOURCES = ["frontend_kernels.cu", "frontend_warp.cu", "runtime.cu", "abi.cu", "noalloc.cu"]
+SOURCES = ["frontend_kernels.cu", "frontend_warp.cu", "runtime.cu", "abi.cu", "noalloc.cu", "server.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",

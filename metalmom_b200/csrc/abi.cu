@@ -254,7 +254,9 @@ int32_t mm_mfcc(mm_context ctx, const float *signal_data, int64_t signal_length,
 // ---------------------------------------------------------------------------
 // additive: batches and plans
 // ---------------------------------------------------------------------------
-static int resolve_frontend(const MMFrontEndParams *p, Group &g) {
+}  // extern "C"
+
+int mm::resolve_frontend(const MMFrontEndParams *p, Group &g) {
   if (!p) return MM_ERR_INVALID_INPUT;
   int st = resolve_mel_group(g, p->sample_rate, p->n_fft, p->hop_length, p->win_length, p->center,
                              p->n_mels, p->f_min, p->f_max);
@@ -271,6 +273,8 @@ static int resolve_frontend(const MMFrontEndParams *p, Group &g) {
   g.n_mfcc_eff = std::min(p->n_mfcc, p->n_mels);
   return MM_OK;
 }
+
+extern "C" {
 
 int32_t mm_mfcc_batch(mm_context ctx, const float *const *signals, const int64_t *lengths,
                       int32_t n_clips, const MMFrontEndParams *params, MMBuffer *outs) {

@@ -41,6 +41,10 @@ long long frame_count(long long length, int n_fft, int hop, int center);
 // Rows of one clip's output block for the group's mode.
 int output_rows(const Group &g);
 
+// MFCC-path group from MMFrontEndParams (sentinels of mm_mfcc, pad mode,
+// top_db); MM_ERR_INVALID_INPUT for unsupported values.
+int resolve_frontend(const MMFrontEndParams *p, Group &g);
+
 // Resident tables for (device, sr, n_fft, win, n_mels, fmin, fmax, n_mfcc).
 const DevTables *get_tables(const Group &g, int *status);
 

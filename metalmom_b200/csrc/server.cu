@@ -1,0 +1,484 @@
+// Serving engine of libmetalmom.so (mm_server_*): continuous batching of MFCC
+// requests with device-memory admission.  No counterpart in the reference,
+// which computes one clip per call (Bridge.swift:402 mm_mfcc).
+//
+// One scheduler thread per server:
+//   * submit() copies the request's samples and queues it (any thread);
+//   * whenever one of `max_inflight` stream slots is free, the scheduler
+//     takes the oldest pending request and every other pending request of
+//     the same parameter group (FIFO, up to max_batch_clips and the free part
+//     of the device budget), copies them into the slot's pinned staging
+//     buffer, and enqueues H2D -> frame kernel -> DCT -> D2H on the slot's
+//     stream with a stream-ordered device arena (cudaMallocAsync);
+//   * a host callback at the end of the stream marks the batch finished; the
+//     scheduler then hands each request its result, releases the arena and
+//     the budget, and refills the slot with whatever arrived meanwhile.
+// Requests that arrive while batches run are therefore admitted as slots and
+// memory free up, and batches of different groups run concurrently.
+// Filterbanks and other tables stay resident per group (get_tables).
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+#include "runtime.h"
+
+using namespace mm;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
+
+struct Request {
+  int64_t id = 0;
+  Group g;
+  std::vector<float> signal;
+  float *result = nullptr;  // malloc'd [rows x frames], handed to the caller
+  long long rows = 0, frames = 0;
+  int state = REQ_PENDING;
+  int status = MM_OK;
+  Clock::time_point t_submit, t_done;
+};
+
+// Requests batch together when every launch parameter agrees.
+bool same_group(const Group &a, const Group &b) {
+  return std::tie(a.sr, a.n_fft, a.hop, a.win, a.center, a.pad_mode, a.n_mels, a.n_mfcc_eff, a.fmin, a.fmax,
+                  a.top_db) == std::tie(b.sr, b.n_fft, b.hop, b.win, b.center, b.pad_mode, b.n_mels,
+                                        b.n_mfcc_eff, b.fmin, b.fmax, b.top_db);
+}
+
+struct Server;
+
+struct Slot {
+  Server *srv = nullptr;
+  cudaStream_t stream = nullptr;
+  char *pinned = nullptr;
+  size_t pinned_bytes = 0;
+  // current batch
+  bool busy = false;
+  std::atomic<bool> finished{false};
+  std::vector<Request *> reqs;
+  Group g;
+  Layout L;
+  char *arena = nullptr;
+  size_t arena_size = 0;
+  size_t sig_bytes = 0, desc_bytes = 0, out_bytes = 0;
+  int error = MM_OK;
+};
+
+struct Server {
+  int device = 0;
+  size_t budget = 0;
+  int max_batch = 256;
+  std::vector<Slot *> slots;
+
+  std::mutex mu;
+  std::condition_variable cv;       // wakes the scheduler
+  std::condition_variable done_cv;  // wakes waiters
+  std::deque<Request *> pending;
+  std::unordered_map<int64_t, Request *> reqs;
+  int64_t next_id = 1;
+  bool stop = false;
+  std::thread worker;
+
+  // accounting (under mu)
+  size_t in_use = 0, peak = 0;
+  int64_t submitted = 0, completed = 0, failed = 0, batches = 0;
+  double audio_s = 0.0;
+  std::vector<double> lat_ms;
+
+  void run();
+  bool admit_one(std::unique_lock<std::mutex> &lk);
+  void finish(Slot *s);
+};
+
+void CUDART_CB on_stream_done(void *p) {
+  Slot *s = static_cast<Slot *>(p);
+  Server *srv = s->srv;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    s->finished.store(true);
+  }
+  srv->cv.notify_all();
+}
+
+// Take the next batch out of `pending` and launch it on a free slot.
+// Returns false when nothing could be launched (no slot, nothing pending,
+// or the head of the queue waits for memory).  Called with mu held; drops it
+// while copying and enqueueing.
+bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
+  Slot *slot = nullptr;
+  for (Slot *s : slots)
+    if (!s->busy) {
+      slot = s;
+      break;
+    }
+  if (!slot || pending.empty()) return false;
+
+  Request *head = pending.front();
+  const Group g0 = head->g;
+  // FIFO scan: the head and the following requests of its group, while the
+  // batch's arena fits in the free budget.
+  std::vector<Request *> take;
+  std::vector<int64_t> lens;
+  Layout L;
+  size_t bytes = 0;
+  Group g = g0;
+  g.variant = group_variant(g);
+  for (Request *r : pending) {
+    if ((int)take.size() >= max_batch) break;
+    if (!same_group(r->g, g0)) continue;
+    lens.push_back((int64_t)r->signal.size());
+    Layout trial;
+    make_layout(g, lens.data(), (int)lens.size(), trial);
+    const size_t need = arena_bytes(g, trial);
+    if (in_use + need > budget) {
+      lens.pop_back();
+      break;
+    }
+    take.push_back(r);
+    L = std::move(trial);
+    bytes = need;
+  }
+  if (take.empty()) {
+    bool any_busy = false;
+    for (Slot *s : slots) any_busy |= s->busy;
+    if (any_busy) return false;  // wait for memory to free up
+    // nothing runs and the request alone exceeds the budget: it can never run
+    pending.pop_front();
+    head->state = REQ_FAILED;
+    head->status = MM_ERR_ALLOC_FAILED;
+    head->t_done = Clock::now();
+    failed++;
+    done_cv.notify_all();
+    return true;
+  }
+  for (Request *r : take) {
+    r->state = REQ_RUNNING;
+    pending.erase(std::find(pending.begin(), pending.end(), r));
+  }
+  slot->busy = true;
+  slot->finished.store(false);
+  slot->reqs = take;
+  slot->g = g;
+  slot->L = std::move(L);
+  slot->arena_size = bytes;
+  slot->error = MM_OK;
+  in_use += bytes;
+  peak = std::max(peak, in_use);
+  batches++;
+
+  // ---- outside the lock: staging copies and the launch sequence
+  lk.unlock();
+  int st = MM_OK;
+  const DevTables *t = get_tables(g, &st);
+  cudaError_t e = cudaSuccess;
+  if (st == MM_OK) {
+    DevBatch probe;
+    slot->desc_bytes = carve_arena(g, slot->L, nullptr, probe);
+    slot->sig_bytes = sizeof(float) * (size_t)slot->L.sig_elems;
+    slot->out_bytes = sizeof(float) * (size_t)slot->L.out_elems;
+    const size_t host_need = std::max(slot->sig_bytes + slot->desc_bytes, slot->out_bytes) + 256;
+    if (host_need > slot->pinned_bytes) {
+      if (slot->pinned) cudaFreeHost(slot->pinned);
+      slot->pinned = nullptr;
+      slot->pinned_bytes = 0;
+      e = cudaMallocHost(&slot->pinned, host_need + host_need / 4);
+      if (e == cudaSuccess) slot->pinned_bytes = host_need + host_need / 4;
+    }
+    if (e == cudaSuccess) e = cudaMallocAsync(&slot->arena, bytes, slot->stream);
+    if (e == cudaSuccess) {
+      char *h = slot->pinned;
+      for (size_t i = 0; i < take.size(); i++)
+        memcpy(h + sizeof(float) * (size_t)slot->L.clips[i].sig_off, take[i]->signal.data(),
+               sizeof(float) * take[i]->signal.size());
+      pack_descriptors(slot->L, h + slot->sig_bytes);
+      DevBatch b;
+      carve_arena(g, slot->L, slot->arena, b);
+      e = cudaMemcpyAsync(b.signal, h, slot->sig_bytes, cudaMemcpyHostToDevice, slot->stream);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b.clips, h + slot->sig_bytes, slot->desc_bytes, cudaMemcpyHostToDevice, slot->stream);
+      if (e == cudaSuccess) e = enqueue_batch(g, slot->L, t, b, slot->stream, nullptr, nullptr);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h, b.out, slot->out_bytes, cudaMemcpyDeviceToHost, slot->stream);
+    }
+    if (e != cudaSuccess) st = cuda_status(e);
+  }
+  if (st != MM_OK) {
+    cudaGetLastError();
+    slot->error = st;
+  }
+  // The callback also runs after a failed enqueue so that the batch is reaped.
+  e = cudaLaunchHostFunc(slot->stream, on_stream_done, slot);
+  lk.lock();
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    slot->error = cuda_status(e);
+    slot->finished.store(true);
+  }
+  return true;
+}
+
+// Hand out the results of a finished batch (called with mu held).
+void Server::finish(Slot *s) {
+  const auto now = Clock::now();
+  const int rows = output_rows(s->g);
+  for (size_t i = 0; i < s->reqs.size(); i++) {
+    Request *r = s->reqs[i];
+    r->t_done = now;
+    r->rows = rows;
+    r->frames = s->L.clips[i].n_frames;
+    if (s->error != MM_OK) {
+      r->state = REQ_FAILED;
+      r->status = s->error;
+      failed++;
+      continue;
+    }
+    const size_t cnt = (size_t)rows * (size_t)r->frames;
+    if (cnt) {
+      r->result = (float *)malloc(sizeof(float) * cnt);
+      if (!r->result) {
+        r->state = REQ_FAILED;
+        r->status = MM_ERR_ALLOC_FAILED;
+        failed++;
+        continue;
+      }
+      memcpy(r->result, s->pinned + sizeof(float) * (size_t)s->L.clips[i].out_off, sizeof(float) * cnt);
+    }
+    r->state = REQ_DONE;
+    r->status = MM_OK;
+    completed++;
+    audio_s += (double)r->signal.size() / (double)r->g.sr;
+    lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+    std::vector<float>().swap(r->signal);
+  }
+  if (s->arena) cudaFreeAsync(s->arena, s->stream);
+  s->arena = nullptr;
+  in_use -= s->arena_size;
+  s->arena_size = 0;
+  s->reqs.clear();
+  s->busy = false;
+  done_cv.notify_all();
+}
+
+void Server::run() {
+  cudaSetDevice(device);
+  std::unique_lock<std::mutex> lk(mu);
+  for (;;) {
+    bool any_busy = false;
+    for (Slot *s : slots) {
+      if (s->busy && s->finished.load()) finish(s);
+      any_busy |= s->busy;
+    }
+    if (stop && !any_busy) break;
+    bool launched = false;
+    if (!stop)
+      while (admit_one(lk)) launched = true;
+    if (launched) continue;
+    cv.wait(lk);
+  }
+}
+
+// Moves a finished request's result into *out (or returns its error) and
+// forgets the request.  Called with mu held.
+int32_t deliver(Server *srv, Request *r, MMBuffer *out) {
+  const int32_t st = r->status;
+  if (r->state == REQ_DONE) {
+    fill_buffer(out, r->result, r->rows, r->frames);
+    r->result = nullptr;
+  }
+  srv->reqs.erase(r->id);
+  free(r->result);
+  delete r;
+  return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+mm_server mm_server_create(const MMServerConfig *cfg, int32_t *status) {
+  int dummy;
+  int32_t *st = status ? status : &dummy;
+  *st = gpu_available();
+  if (*st != MM_OK) return nullptr;
+  Server *srv = new (std::nothrow) Server();
+  if (!srv) {
+    *st = MM_ERR_ALLOC_FAILED;
+    return nullptr;
+  }
+  const int64_t budget = (cfg && cfg->device_budget_bytes > 0) ? cfg->device_budget_bytes : (40LL << 30);
+  const int inflight = (cfg && cfg->max_inflight > 0) ? std::min(cfg->max_inflight, 64) : 4;
+  srv->budget = (size_t)budget;
+  srv->max_batch = (cfg && cfg->max_batch_clips > 0) ? cfg->max_batch_clips : 256;
+  cudaGetDevice(&srv->device);
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < inflight && e == cudaSuccess; i++) {
+    Slot *s = new Slot();
+    s->srv = srv;
+    e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    srv->slots.push_back(s);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    for (Slot *s : srv->slots) {
+      if (s->stream) cudaStreamDestroy(s->stream);
+      delete s;
+    }
+    delete srv;
+    *st = cuda_status(e);
+    return nullptr;
+  }
+  srv->worker = std::thread([srv] { srv->run(); });
+  *st = MM_OK;
+  return srv;
+}
+
+void mm_server_destroy(mm_server server) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv) return;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stop = true;
+    for (Request *r : srv->pending) {  // never started
+      r->state = REQ_FAILED;
+      r->status = MM_ERR_INVALID_INPUT;
+    }
+    srv->pending.clear();
+  }
+  srv->cv.notify_all();
+  if (srv->worker.joinable()) srv->worker.join();  // in-flight batches finish first
+  for (Slot *s : srv->slots) {
+    if (s->stream) {
+      cudaStreamSynchronize(s->stream);
+      cudaStreamDestroy(s->stream);
+    }
+    if (s->pinned) cudaFreeHost(s->pinned);
+    delete s;
+  }
+  for (auto &kv : srv->reqs) {
+    free(kv.second->result);
+    delete kv.second;
+  }
+  delete srv;
+}
+
+int32_t mm_server_submit(mm_server server, const float *signal, int64_t length, const MMFrontEndParams *params,
+                         int64_t *request_id) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv || !signal || length <= 0 || !request_id) return MM_ERR_INVALID_INPUT;
+  Request *r = new (std::nothrow) Request();
+  if (!r) return MM_ERR_ALLOC_FAILED;
+  int st = resolve_frontend(params, r->g);
+  if (st == MM_OK && (r->g.n_mfcc_eff <= 0 || frame_count(length, r->g.n_fft, r->g.hop, r->g.center) == 0))
+    st = MM_ERR_INVALID_INPUT;  // nothing to compute: callers use mm_mfcc for empty shapes
+  if (st != MM_OK) {
+    delete r;
+    return st;
+  }
+  try {
+    r->signal.assign(signal, signal + length);
+  } catch (...) {
+    delete r;
+    return MM_ERR_ALLOC_FAILED;
+  }
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stop) {
+      delete r;
+      return MM_ERR_INVALID_INPUT;
+    }
+    r->id = srv->next_id++;
+    srv->reqs[r->id] = r;
+    srv->pending.push_back(r);
+    srv->submitted++;
+    *request_id = r->id;
+  }
+  srv->cv.notify_all();
+  return MM_OK;
+}
+
+int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer *out) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv || !out) return MM_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(request_id);
+  if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
+  Request *r = it->second;
+  if (r->state == REQ_PENDING || r->state == REQ_RUNNING) return MM_PENDING;
+  return deliver(srv, r, out);
+}
+
+int32_t mm_server_wait(mm_server server, int64_t request_id, int32_t timeout_ms, MMBuffer *out) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv || !out) return MM_ERR_INVALID_INPUT;
+  std::unique_lock<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(request_id);
+  if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
+  Request *r = it->second;
+  auto ready = [r] { return r->state == REQ_DONE || r->state == REQ_FAILED; };
+  if (timeout_ms < 0) srv->done_cv.wait(lk, ready);
+  else if (!srv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return MM_PENDING;
+  return deliver(srv, r, out);
+}
+
+int32_t mm_server_stats(mm_server server, MMServerStats *out) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv || !out) return MM_ERR_INVALID_INPUT;
+  std::vector<double> lat;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    out->submitted = srv->submitted;
+    out->completed = srv->completed;
+    out->failed = srv->failed;
+    out->pending = (int64_t)srv->pending.size();
+    int64_t busy = 0;
+    for (Slot *s : srv->slots) busy += s->busy ? 1 : 0;
+    out->inflight_batches = busy;
+    out->batches_launched = srv->batches;
+    out->bytes_in_use = (int64_t)srv->in_use;
+    out->peak_bytes_in_use = (int64_t)srv->peak;
+    out->audio_seconds_completed = srv->audio_s;
+    lat = srv->lat_ms;
+  }
+  out->latency_p50_ms = out->latency_p99_ms = out->latency_mean_ms = out->latency_max_ms = 0.0;
+  if (!lat.empty()) {
+    std::sort(lat.begin(), lat.end());
+    auto pct = [&lat](double p) {
+      const size_t i = (size_t)std::min<double>((double)(lat.size() - 1), p * (double)(lat.size() - 1) + 0.5);
+      return lat[i];
+    };
+    double sum = 0.0;
+    for (double v : lat) sum += v;
+    out->latency_p50_ms = pct(0.50);
+    out->latency_p99_ms = pct(0.99);
+    out->latency_mean_ms = sum / (double)lat.size();
+    out->latency_max_ms = lat.back();
+  }
+  return MM_OK;
+}
+
+int32_t mm_server_reset_stats(mm_server server) {
+  Server *srv = static_cast<Server *>(server);
+  if (!srv) return MM_ERR_INVALID_INPUT;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  srv->submitted = srv->completed = srv->failed = srv->batches = 0;
+  srv->audio_s = 0.0;
+  srv->lat_ms.clear();
+  srv->peak = srv->in_use;
+  return MM_OK;
+}
+
+}  // extern "C"

@@ -115,3 +115,5 @@ def test_no_gpu_is_reported_not_hidden():
             fn()
     with pytest.raises(RuntimeError, match="status -2"):
         M.Plan([4096, 5000])
+    with pytest.raises(RuntimeError, match="status -2"):
+        M.Server()

@@ -161,6 +161,134 @@ def baseline_leg(plan, clips, world, args):
     return out
 
 
+# ---------------------------------------------------------------------------
+# served stream: Poisson arrivals, log-normal clip lengths (median 8 s,
+# sigma 1, clipped to 0.5-300 s), parameter group drawn uniformly from the
+# single-clip music front end, the uneven-batch groups and the speech front
+# end; 40 GB admission budget
+# ---------------------------------------------------------------------------
+SERVE_MUSIC = dict(sr=22050, n_fft=2048, hop_length=512, n_mels=128, n_mfcc=20)
+SERVE_SPEECH = dict(sr=16000, n_fft=512, hop_length=160, win_length=400, n_mels=80, n_mfcc=13,
+                    fmin=20.0, fmax=8000.0)
+
+
+def serve_group(rng):
+    k = int(rng.integers(3))
+    if k == 0:
+        return SERVE_MUSIC
+    if k == 2:
+        return SERVE_SPEECH
+    n_fft = int(rng.choice([1024, 2048, 4096]))
+    return dict(sr=int(rng.choice([22050, 44100])), n_fft=n_fft, hop_length=n_fft // 4,
+                n_mels=int(rng.choice([64, 128])), n_mfcc=20)
+
+
+def serve_pools():
+    from metalmom_b200 import synth
+    return {22050: synth.music_clip(300 * 22050, 22050, seed=71),
+            44100: synth.music_clip(300 * 44100, 44100, seed=72),
+            16000: synth.speech_clip(300 * 16000, 16000, seed=73)}
+
+
+def serve_requests(pools, rate, duration, seed):
+    """(arrival time, clip, params) of a Poisson stream; clips are windows of
+    long seeded clips."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            return out
+        g = serve_group(rng)
+        secs = float(np.clip(rng.lognormal(np.log(8.0), 1.0), 0.5, 300.0))
+        pool = pools[g["sr"]]
+        n = int(secs * g["sr"])
+        start = int(rng.integers(0, len(pool) - n + 1))
+        out.append((t, pool[start:start + n], g))
+
+
+def _pcts(lat_ms):
+    lat = np.sort(np.asarray(lat_ms))
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+def serving_leg(duration=3.0, rates=(50, 500, 2000), burst=2000, plain_s=2.0):
+    """Continuous batching (Server) on open-loop Poisson streams, a burst for
+    the sustained rate, and the plain per-request form (mm_mfcc per request,
+    in arrival order) on the same kind of stream."""
+    import metalmom_b200 as M
+    pools = serve_pools()
+    res = {"workload": "Poisson arrivals; lengths log-normal (median 8 s, sigma 1) in 0.5-300 s; "
+                       "group uniform over {30 s-clip music front end, uneven-batch groups "
+                       "(sr 22050/44100, n_fft 1024/2048/4096, 64/128 mels), speech front end "
+                       "(16 kHz, n_fft 512, win 400, hop 160, 80 mels, 13 MFCC)}",
+           "budget_bytes": 40 << 30, "streams": []}
+    with M.Server(budget_bytes=40 << 30, max_batch_clips=256, max_inflight=4) as srv:
+        # one request per parameter group first: tables are built once per group
+        groups = [SERVE_MUSIC, SERVE_SPEECH] + [
+            dict(sr=sr, n_fft=nf, hop_length=nf // 4, n_mels=nm, n_mfcc=20)
+            for sr in (22050, 44100) for nf in (1024, 2048, 4096) for nm in (64, 128)]
+        for rid in [srv.submit(pools[g["sr"]][:5 * g["sr"]], **g) for g in groups]:
+            srv.result(rid)
+        warm = serve_requests(pools, 200, 0.5, seed=9)
+        for rid in [srv.submit(y, **g) for _, y, g in warm]:
+            srv.result(rid)
+        for rate in rates:
+            reqs = serve_requests(pools, rate, duration, seed=rate)
+            srv.reset_stats()
+            t0 = time.perf_counter()
+            ids = []
+            for t, y, g in reqs:
+                while time.perf_counter() - t0 < t:
+                    dt = t - (time.perf_counter() - t0)
+                    if dt > 0.002:
+                        time.sleep(dt - 0.001)
+                ids.append(srv.submit(y, **g))
+            for rid in ids:
+                srv.result(rid)
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            res["streams"].append({
+                "rate_req_s": rate, "requests": len(reqs), "p50_ms": st["latency_p50_ms"],
+                "p99_ms": st["latency_p99_ms"], "max_ms": st["latency_max_ms"],
+                "audio_hours_per_s": st["audio_seconds_completed"] / 3600.0 / wall,
+                "batches": st["batches_launched"], "failed": st["failed"],
+                "peak_device_bytes": st["peak_bytes_in_use"]})
+        reqs = serve_requests(pools, burst / 0.001, 1.0, seed=4242)[:burst]
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        ids = [srv.submit(y, **g) for _, y, g in reqs]
+        for rid in ids:
+            srv.result(rid)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        res["burst"] = {"requests": len(reqs), "audio_hours_per_s": st["audio_seconds_completed"] / 3600.0 / wall,
+                        "p50_ms": st["latency_p50_ms"], "p99_ms": st["latency_p99_ms"],
+                        "batches": st["batches_launched"]}
+    # the plain per-request form on a stream it can follow
+    rate = 50
+    reqs = serve_requests(pools, rate, plain_s, seed=77)
+    for _, y, g in reqs[:3]:
+        M.mfcc(y, **g)
+    lat, audio = [], 0.0
+    t0 = time.perf_counter()
+    for t, y, g in reqs:
+        while time.perf_counter() - t0 < t:
+            time.sleep(0.0002)
+        M.mfcc(y, **g)
+        lat.append((time.perf_counter() - t0 - t) * 1e3)
+        audio += len(y) / g["sr"]
+    wall = time.perf_counter() - t0
+    p50, p99 = _pcts(lat)
+    res["plain_per_request"] = {"rate_req_s": rate, "requests": len(reqs), "p50_ms": p50, "p99_ms": p99,
+                                "audio_hours_per_s": audio / 3600.0 / wall,
+                                "api": "mm_mfcc per request in arrival order (host in/out)"}
+    ab = [s for s in res["streams"] if s["rate_req_s"] == rate]
+    if ab:
+        res["plain_vs_server_p99"] = p99 / ab[0]["p99_ms"] if ab[0]["p99_ms"] > 0 else None
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import metalmom_b200 as M
@@ -291,7 +419,10 @@ def run_ours(args, rank, world, local_rank):
         pipe_bytes = 4.0 * sum(lengths) + 4.0 * N_MFCC * T_total
         flops_fft = 2.5 * N_FFT * np.log2(N_FFT) * T_total
         traffic = None
-        tp = os.path.join(ROOT, "profiles", "frontend_kernel_256clips_traffic.txt")
+        warp = tune["best"] == 3
+        kname = "frame_warp_kernel<11>" if warp else f"frontend_kernel<11,V{tune['best']},MELDB>"
+        tp = os.path.join(ROOT, "profiles", ("frame_warp_kernel" if warp else "frontend_kernel")
+                          + "_256clips_traffic.txt")
         if os.path.exists(tp) and n_clips == N_CLIPS:
             for line in open(tp):
                 if line.startswith("bytes_per_launch:"):
@@ -301,7 +432,7 @@ def run_ours(args, rank, world, local_rank):
             "warmup": W, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded music-like clips)",
             "config": dict(workload_config(n_clips), parallelism=f"clip-sharded x{world}" if world > 1 else "1 GPU"),
-            "roofline": {"bound": "hbm", "kernel": "frontend_kernel<11,V,MELDB>",
+            "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": peak_note, "traffic": traffic,
                          "kernel_ms": frame_ms, "dct_ms": dct_ms,
@@ -321,6 +452,8 @@ def run_ours(args, rank, world, local_rank):
         }
         if not args.no_cpu:
             result.update(baseline_leg(plan, clips, world, args))
+        if not args.no_serve:
+            result["serving"] = serving_leg()
     plan.close()
     if dist is not None:
         dist.barrier()
@@ -371,6 +504,7 @@ def main():
     ap.add_argument("--cpu-clips", type=int, default=128)
     ap.add_argument("--ref-clips", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))

@@ -197,6 +197,7 @@ typedef struct {
     int64_t device_budget_bytes; /* device memory of the batches in flight; <= 0: 40 GiB */
     int32_t max_batch_clips;     /* <= 0: 256 */
     int32_t max_inflight;        /* batches on the device at once; <= 0: 4 (at most 64) */
+    int64_t host_pinned_bytes;   /* pinned host memory for queued samples; <= 0: 8 GiB */
 } MMServerConfig;
 
 typedef struct {
@@ -204,13 +205,15 @@ typedef struct {
     int64_t bytes_in_use, peak_bytes_in_use;
     double audio_seconds_completed;
     double latency_p50_ms, latency_p99_ms, latency_mean_ms, latency_max_ms; /* submit -> result */
+    double scheduler_launch_ms, scheduler_finish_ms; /* host time spent starting / reaping batches */
 } MMServerStats;
 
 MM_API mm_server mm_server_create(const MMServerConfig* config, int32_t* status);
 /* Finishes the batches in flight, drops requests that never started and
  * frees every undelivered result. */
 MM_API void mm_server_destroy(mm_server server);
-/* Copies the samples; *request_id identifies the request.  A request with no
+/* Copies the samples (into pinned host memory while the pool has room);
+ * *request_id identifies the request.  A request with no
  * frame or no coefficient is rejected (MM_ERR_INVALID_INPUT); a request
  * whose batch alone exceeds the budget fails with MM_ERR_ALLOC_FAILED. */
 MM_API int32_t mm_server_submit(mm_server server, const float* signal, int64_t length,

@@ -21,6 +21,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "fft_radix.cuh"
 #include "frame_common.cuh"
@@ -954,21 +957,52 @@ static int sm_count() {
   return sms;
 }
 
+// Launch geometry of a persistent kernel, cached per (device, kernel, threads,
+// dynamic shared memory), so that a launch costs no extra driver calls.  The
+// kernel's shared-memory opt-in is one value per (device, kernel): it is only
+// ever raised, so every size cached before stays launchable.
+cudaError_t persistent_geometry(const void *kern, int threads, size_t smem, int *per_sm, int *sms) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, const void *, int, size_t>, std::pair<int, int>> cache;
+  static std::map<std::pair<int, const void *>, size_t> opted_in;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const auto key = std::make_tuple(dev, kern, threads, smem);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(key);
+  if (it != cache.end()) {
+    *per_sm = it->second.first;
+    *sms = it->second.second;
+    return cudaSuccess;
+  }
+  size_t &opt = opted_in[std::make_pair(dev, kern)];
+  if (smem > 48 * 1024 && smem > opt) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    opt = smem;
+  }
+  int p = 0, n = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  if (p < 1) return cudaErrorInvalidConfiguration;
+  cache[key] = {p, n};
+  *per_sm = p;
+  *sms = n;
+  return cudaSuccess;
+}
+
 template <bool TINY, typename K>
 static cudaError_t launch_persistent(K kern, int threads, size_t smem, int tiles, int grid_limit,
                                      size_t *configured, const FrontArgs &a, cudaStream_t s,
                                      int *launched, int n_fft) {
-  cudaError_t e;
-  if (smem > 48 * 1024 && smem > *configured) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    *configured = smem;
-  }
-  int per_sm = 1;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  (void)configured;
+  int per_sm = 1, sms = 148;
+  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(kern), threads, smem, &per_sm, &sms);
   if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  long long grid = (long long)sm_count() * per_sm;
+  long long grid = (long long)sms * per_sm;
   if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
   if (grid > tiles) grid = tiles;
   if (grid < 1) return cudaSuccess;
@@ -1046,7 +1080,9 @@ cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a
 
 template <int KQ>
 static cudaError_t launch_dct_t(const DctArgs &a, cudaStream_t s) {
-  long long grid = (long long)sm_count() * 4;
+  static int sms = 0;
+  if (sms == 0) sms = sm_count();
+  long long grid = (long long)sms * 4;
   if (grid > a.total_tiles) grid = a.total_tiles;
   dct_kernel<KQ><<<(unsigned)grid, 256, 0, s>>>(a);
   return cudaGetLastError();

@@ -508,32 +508,17 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
 }
 
-static int sm_count_w() {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return sms;
-}
-
 template <int LOG2N>
 static cudaError_t launch_warp_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using S = WShape<LOG2N>;
   const size_t split_bytes = align16(8 * (size_t)(S::M + 1));
   const size_t smem = warp_fixed_smem<LOG2N>() + 16 * (size_t)(a.n_mels + 1) +
                       std::max(split_bytes, mel_smem_bytes(0, a.mel_nnz));
-  static size_t configured = 0;
   auto kern = frame_warp_kernel<LOG2N>;
-  cudaError_t e;
-  if (smem > 48 * 1024 && smem > configured) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = smem;
-  }
-  int per_sm = 1;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, S::THREADS, smem);
+  int per_sm = 1, sms = 148;
+  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(kern), S::THREADS, smem, &per_sm, &sms);
   if (e != cudaSuccess) return e;
-  if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  long long grid = (long long)sm_count_w() * per_sm;
+  long long grid = (long long)sms * per_sm;
   if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
   if (grid > a.total_tiles) grid = a.total_tiles;
   if (grid < 1) return cudaSuccess;

@@ -106,6 +106,9 @@ cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, 
                             int win, int n_mels, float fmin, float fmax, int n_mfcc_eff, int window_zero,
                             cudaStream_t s);
 
+// Blocks per SM and SM count for a persistent launch of `kern` (cached).
+cudaError_t persistent_geometry(const void *kern, int threads, size_t smem, int *per_sm, int *sms);
+
 // Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
 cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,
                             cudaStream_t s, int *launched_grid);

@@ -3,13 +3,14 @@
 // which computes one clip per call (Bridge.swift:402 mm_mfcc).
 //
 // One scheduler thread per server:
-//   * submit() copies the request's samples and queues it (any thread);
+//   * submit() copies the request's samples into a pinned block from the
+//     server's pinned pool (the only host copy of the samples) and queues it;
 //   * whenever one of `max_inflight` stream slots is free, the scheduler
 //     takes the oldest pending request and every other pending request of
 //     the same parameter group (FIFO, up to max_batch_clips and the free part
-//     of the device budget), copies them into the slot's pinned staging
-//     buffer, and enqueues H2D -> frame kernel -> DCT -> D2H on the slot's
-//     stream with a stream-ordered device arena (cudaMallocAsync);
+//     of the device budget) and enqueues H2D of each pinned block -> frame
+//     kernel -> DCT -> D2H on the slot's stream, with a stream-ordered device
+//     arena (cudaMallocAsync);
 //   * a host callback at the end of the stream marks the batch finished; the
 //     scheduler then hands each request its result, releases the arena and
 //     the budget, and refills the slot with whatever arrived meanwhile.
@@ -40,10 +41,80 @@ using Clock = std::chrono::steady_clock;
 
 enum ReqState { REQ_PENDING = 0, REQ_RUNNING = 1, REQ_DONE = 2, REQ_FAILED = 3 };
 
+// Pinned host blocks in power-of-two size classes, carved from 256 MiB chunks
+// that stay allocated until the server is destroyed (freeing pinned memory
+// would synchronise the device).  get() returns null when the pinned total
+// would exceed the cap; the request then keeps a pageable copy.
+class PinnedPool {
+ public:
+  static constexpr size_t kChunk = size_t(256) << 20;
+  explicit PinnedPool(size_t cap) : cap_(cap) {}
+  ~PinnedPool() {
+    for (char *c : chunks_) cudaFreeHost(c);
+  }
+  static int size_class(size_t bytes) {
+    int c = 12;
+    while ((size_t(1) << c) < bytes) c++;
+    return c;
+  }
+  float *get(size_t bytes, int *cls) {
+    const int c = size_class(bytes);
+    const size_t sz = size_t(1) << c;
+    std::lock_guard<std::mutex> lk(mu_);
+    *cls = c;
+    if (!free_[c].empty()) {
+      char *p = free_[c].back();
+      free_[c].pop_back();
+      return reinterpret_cast<float *>(p);
+    }
+    if (sz > kChunk) {  // a block of its own
+      if (total_ + sz > cap_) return nullptr;
+      char *p = nullptr;
+      if (cudaMallocHost(&p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+      chunks_.push_back(p);
+      total_ += sz;
+      return reinterpret_cast<float *>(p);
+    }
+    if (left_ < sz) {
+      if (total_ + kChunk > cap_) return nullptr;
+      char *p = nullptr;
+      if (cudaMallocHost(&p, kChunk) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+      chunks_.push_back(p);
+      total_ += kChunk;
+      cur_ = p;
+      left_ = kChunk;
+    }
+    char *p = cur_;
+    cur_ += sz;
+    left_ -= sz;
+    return reinterpret_cast<float *>(p);
+  }
+  void put(float *p, int cls) {
+    std::lock_guard<std::mutex> lk(mu_);
+    free_[cls].push_back(reinterpret_cast<char *>(p));
+  }
+
+ private:
+  std::mutex mu_;
+  std::vector<char *> chunks_;
+  std::vector<char *> free_[64];
+  char *cur_ = nullptr;
+  size_t left_ = 0, total_ = 0, cap_;
+};
+
 struct Request {
   int64_t id = 0;
   Group g;
-  std::vector<float> signal;
+  long long length = 0;
+  float *pin = nullptr;      // samples in a pinned block (pin_cls = its size class) ...
+  int pin_cls = 0;
+  std::vector<float> signal;  // ... or, when the pinned pool is full, a pageable copy
   float *result = nullptr;  // malloc'd [rows x frames], handed to the caller
   long long rows = 0, frames = 0;
   int state = REQ_PENDING;
@@ -80,6 +151,8 @@ struct Slot {
 struct Server {
   int device = 0;
   size_t budget = 0;
+  PinnedPool *pool = nullptr;
+  cudaMemPool_t mempool = nullptr;  // device arenas; keeps freed memory for reuse
   int max_batch = 256;
   std::vector<Slot *> slots;
 
@@ -96,6 +169,7 @@ struct Server {
   size_t in_use = 0, peak = 0;
   int64_t submitted = 0, completed = 0, failed = 0, batches = 0;
   double audio_s = 0.0;
+  double launch_ms = 0.0, finish_ms = 0.0;  // scheduler host time per phase
   std::vector<double> lat_ms;
 
   void run();
@@ -132,24 +206,28 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
   // batch's arena fits in the free budget.
   std::vector<Request *> take;
   std::vector<int64_t> lens;
-  Layout L;
-  size_t bytes = 0;
   Group g = g0;
   g.variant = group_variant(g);
+  // per-clip upper bound of the arena (segments are 256-byte aligned)
+  const int F = frames_per_tile(g.log2n, g.variant);
+  const int rows = output_rows(g);
+  size_t bytes = 8 * 256;
   for (Request *r : pending) {
     if ((int)take.size() >= max_batch) break;
     if (!same_group(r->g, g0)) continue;
-    lens.push_back((int64_t)r->signal.size());
-    Layout trial;
-    make_layout(g, lens.data(), (int)lens.size(), trial);
-    const size_t need = arena_bytes(g, trial);
-    if (in_use + need > budget) {
-      lens.pop_back();
-      break;
-    }
+    const long long T = frame_count(r->length, g.n_fft, g.hop, g.center);
+    const size_t need = sizeof(float) * (size_t)((r->length + 3) / 4 * 4) + sizeof(ClipDesc) + 16 +
+                        sizeof(int) * (size_t)((T + F - 1) / F) + 2 * sizeof(int) * (size_t)((T + kDctTile - 1) / kDctTile) +
+                        sizeof(unsigned) + sizeof(float) * (size_t)T * (size_t)(g.n_mels + rows);
+    if (in_use + bytes + need > budget) break;
     take.push_back(r);
-    L = std::move(trial);
-    bytes = need;
+    lens.push_back((int64_t)r->length);
+    bytes += need;
+  }
+  Layout L;
+  if (!take.empty()) {
+    make_layout(g, lens.data(), (int)lens.size(), L);
+    bytes = std::max(bytes, arena_bytes(g, L));
   }
   if (take.empty()) {
     bool any_busy = false;
@@ -179,8 +257,9 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
   peak = std::max(peak, in_use);
   batches++;
 
-  // ---- outside the lock: staging copies and the launch sequence
+  // ---- outside the lock: the launch sequence
   lk.unlock();
+  const auto t_launch = Clock::now();
   int st = MM_OK;
   const DevTables *t = get_tables(g, &st);
   cudaError_t e = cudaSuccess;
@@ -189,7 +268,7 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
     slot->desc_bytes = carve_arena(g, slot->L, nullptr, probe);
     slot->sig_bytes = sizeof(float) * (size_t)slot->L.sig_elems;
     slot->out_bytes = sizeof(float) * (size_t)slot->L.out_elems;
-    const size_t host_need = std::max(slot->sig_bytes + slot->desc_bytes, slot->out_bytes) + 256;
+    const size_t host_need = std::max(slot->desc_bytes, slot->out_bytes) + 256;
     if (host_need > slot->pinned_bytes) {
       if (slot->pinned) cudaFreeHost(slot->pinned);
       slot->pinned = nullptr;
@@ -197,18 +276,19 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
       e = cudaMallocHost(&slot->pinned, host_need + host_need / 4);
       if (e == cudaSuccess) slot->pinned_bytes = host_need + host_need / 4;
     }
-    if (e == cudaSuccess) e = cudaMallocAsync(&slot->arena, bytes, slot->stream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&slot->arena, bytes, mempool, slot->stream);
     if (e == cudaSuccess) {
       char *h = slot->pinned;
-      for (size_t i = 0; i < take.size(); i++)
-        memcpy(h + sizeof(float) * (size_t)slot->L.clips[i].sig_off, take[i]->signal.data(),
-               sizeof(float) * take[i]->signal.size());
-      pack_descriptors(slot->L, h + slot->sig_bytes);
+      pack_descriptors(slot->L, h);
       DevBatch b;
       carve_arena(g, slot->L, slot->arena, b);
-      e = cudaMemcpyAsync(b.signal, h, slot->sig_bytes, cudaMemcpyHostToDevice, slot->stream);
+      for (size_t i = 0; i < take.size() && e == cudaSuccess; i++) {
+        const float *src = take[i]->pin ? take[i]->pin : take[i]->signal.data();
+        e = cudaMemcpyAsync(b.signal + slot->L.clips[i].sig_off, src, sizeof(float) * (size_t)take[i]->length,
+                            cudaMemcpyHostToDevice, slot->stream);
+      }
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b.clips, h + slot->sig_bytes, slot->desc_bytes, cudaMemcpyHostToDevice, slot->stream);
+        e = cudaMemcpyAsync(b.clips, h, slot->desc_bytes, cudaMemcpyHostToDevice, slot->stream);
       if (e == cudaSuccess) e = enqueue_batch(g, slot->L, t, b, slot->stream, nullptr, nullptr);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(h, b.out, slot->out_bytes, cudaMemcpyDeviceToHost, slot->stream);
@@ -221,7 +301,9 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
   }
   // The callback also runs after a failed enqueue so that the batch is reaped.
   e = cudaLaunchHostFunc(slot->stream, on_stream_done, slot);
+  const double dt = std::chrono::duration<double, std::milli>(Clock::now() - t_launch).count();
   lk.lock();
+  launch_ms += dt;
   if (e != cudaSuccess) {
     cudaGetLastError();
     slot->error = cuda_status(e);
@@ -233,6 +315,11 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
 // Hand out the results of a finished batch (called with mu held).
 void Server::finish(Slot *s) {
   const auto now = Clock::now();
+  struct Timer {
+    double *acc;
+    Clock::time_point t0 = Clock::now();
+    ~Timer() { *acc += std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+  } timer{&finish_ms};
   const int rows = output_rows(s->g);
   for (size_t i = 0; i < s->reqs.size(); i++) {
     Request *r = s->reqs[i];
@@ -259,8 +346,12 @@ void Server::finish(Slot *s) {
     r->state = REQ_DONE;
     r->status = MM_OK;
     completed++;
-    audio_s += (double)r->signal.size() / (double)r->g.sr;
+    audio_s += (double)r->length / (double)r->g.sr;
     lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+  }
+  for (Request *r : s->reqs) {  // the samples are on the device (or the batch failed)
+    if (r->pin) pool->put(r->pin, r->pin_cls);
+    r->pin = nullptr;
     std::vector<float>().swap(r->signal);
   }
   if (s->arena) cudaFreeAsync(s->arena, s->stream);
@@ -322,20 +413,37 @@ mm_server mm_server_create(const MMServerConfig *cfg, int32_t *status) {
   const int inflight = (cfg && cfg->max_inflight > 0) ? std::min(cfg->max_inflight, 64) : 4;
   srv->budget = (size_t)budget;
   srv->max_batch = (cfg && cfg->max_batch_clips > 0) ? cfg->max_batch_clips : 256;
+  srv->pool = new PinnedPool((cfg && cfg->host_pinned_bytes > 0) ? (size_t)cfg->host_pinned_bytes
+                                                                 : (size_t(8) << 30));
   cudaGetDevice(&srv->device);
-  cudaError_t e = cudaSuccess;
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = srv->device;
+  cudaError_t e = cudaMemPoolCreate(&srv->mempool, &props);
+  if (e == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;  // never hand freed arenas back to the driver
+    e = cudaMemPoolSetAttribute(srv->mempool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   for (int i = 0; i < inflight && e == cudaSuccess; i++) {
     Slot *s = new Slot();
     s->srv = srv;
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     srv->slots.push_back(s);
+    if (e == cudaSuccess) {  // descriptors + results of a batch; grows if ever needed
+      s->pinned_bytes = size_t(8) << 20;
+      e = cudaMallocHost(&s->pinned, s->pinned_bytes);
+    }
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
     for (Slot *s : srv->slots) {
       if (s->stream) cudaStreamDestroy(s->stream);
+      if (s->pinned) cudaFreeHost(s->pinned);
       delete s;
     }
+    if (srv->mempool) cudaMemPoolDestroy(srv->mempool);
+    delete srv->pool;
     delete srv;
     *st = cuda_status(e);
     return nullptr;
@@ -371,6 +479,8 @@ void mm_server_destroy(mm_server server) {
     free(kv.second->result);
     delete kv.second;
   }
+  if (srv->mempool) cudaMemPoolDestroy(srv->mempool);
+  delete srv->pool;
   delete srv;
 }
 
@@ -387,16 +497,23 @@ int32_t mm_server_submit(mm_server server, const float *signal, int64_t length, 
     delete r;
     return st;
   }
-  try {
-    r->signal.assign(signal, signal + length);
-  } catch (...) {
-    delete r;
-    return MM_ERR_ALLOC_FAILED;
+  r->length = length;
+  r->pin = srv->pool->get(sizeof(float) * (size_t)length, &r->pin_cls);
+  if (r->pin) {
+    memcpy(r->pin, signal, sizeof(float) * (size_t)length);
+  } else {
+    try {
+      r->signal.assign(signal, signal + length);
+    } catch (...) {
+      delete r;
+      return MM_ERR_ALLOC_FAILED;
+    }
   }
   r->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(srv->mu);
     if (srv->stop) {
+      if (r->pin) srv->pool->put(r->pin, r->pin_cls);
       delete r;
       return MM_ERR_INVALID_INPUT;
     }
@@ -451,6 +568,8 @@ int32_t mm_server_stats(mm_server server, MMServerStats *out) {
     out->bytes_in_use = (int64_t)srv->in_use;
     out->peak_bytes_in_use = (int64_t)srv->peak;
     out->audio_seconds_completed = srv->audio_s;
+    out->scheduler_launch_ms = srv->launch_ms;
+    out->scheduler_finish_ms = srv->finish_ms;
     lat = srv->lat_ms;
   }
   out->latency_p50_ms = out->latency_p99_ms = out->latency_mean_ms = out->latency_max_ms = 0.0;
@@ -476,6 +595,7 @@ int32_t mm_server_reset_stats(mm_server server) {
   std::lock_guard<std::mutex> lk(srv->mu);
   srv->submitted = srv->completed = srv->failed = srv->batches = 0;
   srv->audio_s = 0.0;
+  srv->launch_ms = srv->finish_ms = 0.0;
   srv->lat_ms.clear();
   srv->peak = srv->in_use;
   return MM_OK;

@@ -17,7 +17,8 @@ PENDING = lib.MM_PENDING
 
 STAT_KEYS = ["submitted", "completed", "failed", "pending", "inflight_batches", "batches_launched",
              "bytes_in_use", "peak_bytes_in_use", "audio_seconds_completed", "latency_p50_ms",
-             "latency_p99_ms", "latency_mean_ms", "latency_max_ms"]
+             "latency_p99_ms", "latency_mean_ms", "latency_max_ms", "scheduler_launch_ms",
+             "scheduler_finish_ms"]
 
 
 class Server:

@@ -131,32 +131,46 @@ MM_API int32_t mm_mfcc_batch(mm_context ctx, const float* const* signals, const 
 
 /* A plan fixes the parameters and clip lengths of a batch, keeps its tables
  * and device buffers resident and captures its launches in a CUDA graph.
- * Inputs live in one device buffer (clip i at mm_plan_input_offset(i)
- * floats); outputs in another ([rows, n_frames_i] at mm_plan_output_offset).
- * Streams are passed as void* (a cudaStream_t; NULL = the plan's own). */
+ * Clip i's samples go to mm_plan_device_input() + mm_plan_input_offset(i)
+ * floats, its [rows, n_frames_i] result is at mm_plan_device_output() +
+ * mm_plan_output_offset(i) floats.  Streams are passed as void* (a
+ * cudaStream_t; NULL = the plan's own). */
 typedef void* mm_plan;
 
 MM_API mm_plan mm_plan_create(mm_context ctx, const MMFrontEndParams* params,
                        const int64_t* lengths, int32_t n_clips, int32_t* status);
+/* A plan over clips with their own parameters (clip_params[i] for clip i):
+ * clips are grouped by parameter set, each group is cut into branches of at
+ * most max_clips_per_branch clips (0: one branch per group), and the graph
+ * runs the branches concurrently (one persistent launch sequence each, the
+ * autotuned variant of its n_fft).  With host I/O every branch copies its own
+ * clips in and out, so copies of one branch overlap kernels of another. */
+MM_API mm_plan mm_plan_create_groups(mm_context ctx, const MMFrontEndParams* clip_params,
+                                     const int64_t* lengths, int32_t n_clips,
+                                     int32_t max_clips_per_branch, int32_t* status);
+MM_API int32_t mm_plan_branches(mm_plan plan);
+/* Output rows of clip i (min(n_mfcc, n_mels) of its parameters). */
+MM_API int32_t mm_plan_clip_rows(mm_plan plan, int32_t clip);
 MM_API void mm_plan_destroy(mm_plan plan);
 MM_API float* mm_plan_device_input(mm_plan plan);
 MM_API float* mm_plan_device_output(mm_plan plan);
 MM_API int64_t mm_plan_input_offset(mm_plan plan, int32_t clip);
 MM_API int64_t mm_plan_output_offset(mm_plan plan, int32_t clip);
 MM_API int64_t mm_plan_clip_frames(mm_plan plan, int32_t clip);
+/* Output rows shared by every clip, or -1 when the groups differ. */
 MM_API int32_t mm_plan_rows(mm_plan plan);
 MM_API int64_t mm_plan_total_frames(mm_plan plan);
 MM_API int32_t mm_plan_kernel_launches(mm_plan plan);
-/* The log-mel intermediate of the last execution, frame-major
+/* (Plans of one branch.)  The log-mel intermediate of the last execution, frame-major
  * [total_frames, n_mels] (clip i's frames start at the sum of the earlier
  * clips' frame counts), before the top_db floor; and clip i's maximum dB. */
 MM_API float* mm_plan_device_mel_db(mm_plan plan);
 MM_API int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float* max_db);
 /* Replays the captured graph on `stream`. */
 MM_API int32_t mm_plan_execute(mm_plan plan, void* stream);
-/* Same kernels launched directly, with CUDA events recorded around each of
- * the three stages into timing slot `slot` (0..63); read them after the
- * stream has synchronised with mm_plan_stage_ms. */
+/* (Plans of one branch.)  Same kernels launched directly, with CUDA events
+ * recorded around each of the three stages into timing slot `slot` (0..63);
+ * read them after the stream has synchronised with mm_plan_stage_ms. */
 MM_API int32_t mm_plan_execute_timed(mm_plan plan, void* stream, int32_t slot);
 MM_API int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float* ms3);
 /* Host buffers in and out: copies signals[i] into the device input, runs the

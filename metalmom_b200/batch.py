@@ -80,20 +80,39 @@ def mfcc_batch(clips, **params):
 
 
 class Plan:
-    """A resident, graph-captured batch of fixed clip lengths."""
+    """A resident, graph-captured batch of fixed clip lengths.
 
-    def __init__(self, lengths, **params):
+    ``Plan(lengths, **params)``: one parameter set for every clip.
+    ``Plan(lengths, clip_params=[dict, ...], max_clips_per_branch=k)``: each
+    clip with its own parameters; clips are grouped by parameter set and the
+    groups (cut into branches of at most k clips) run as concurrent branches
+    of one graph.
+    """
+
+    def __init__(self, lengths, clip_params=None, max_clips_per_branch=0, **params):
         self.lengths = [int(x) for x in lengths]
-        self._params = frontend_params(**params)
         self._ctx = lib.mm_init()
         st = ffi.new("int32_t*")
         lens = ffi.new("int64_t[]", self.lengths)
-        self._plan = lib.mm_plan_create(self._ctx, self._params, lens, len(self.lengths), st)
+        if clip_params is None:
+            self._params = frontend_params(**params)
+            self._plan = lib.mm_plan_create(self._ctx, self._params, lens, len(self.lengths), st)
+        else:
+            if len(clip_params) != len(self.lengths):
+                lib.mm_destroy(self._ctx)
+                raise ValueError("one parameter dict per clip")
+            self._params = ffi.new("MMFrontEndParams[]", len(clip_params))
+            for i, kw in enumerate(clip_params):
+                self._params[i] = frontend_params(**kw)[0]
+            self._plan = lib.mm_plan_create_groups(self._ctx, self._params, lens, len(self.lengths),
+                                                   int(max_clips_per_branch), st)
         if self._plan == ffi.NULL:
             lib.mm_destroy(self._ctx)
             raise RuntimeError(f"mm_plan_create failed with status {st[0]}")
         self.n = len(self.lengths)
         self.rows = lib.mm_plan_rows(self._plan)
+        self.clip_rows = [lib.mm_plan_clip_rows(self._plan, i) for i in range(self.n)]
+        self.branches = lib.mm_plan_branches(self._plan)
         self.frames = [lib.mm_plan_clip_frames(self._plan, i) for i in range(self.n)]
         self.in_offsets = [lib.mm_plan_input_offset(self._plan, i) for i in range(self.n)]
         self.out_offsets = [lib.mm_plan_output_offset(self._plan, i) for i in range(self.n)]
@@ -137,7 +156,7 @@ class Plan:
         return [ms[0], ms[1], ms[2]]
 
     def alloc_outputs(self):
-        return [np.empty((self.rows, f), dtype=np.float32) for f in self.frames]
+        return [np.empty((r, f), dtype=np.float32) for r, f in zip(self.clip_rows, self.frames)]
 
     def execute_host(self, clips, outs=None, stream: int = 0):
         """Copy ``clips`` in, run, copy MFCCs out (into ``outs`` if given)."""

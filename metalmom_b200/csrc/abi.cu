@@ -294,171 +294,6 @@ int32_t mm_mfcc_batch(mm_context ctx, const float *const *signals, const int64_t
   return MM_OK;
 }
 
-namespace {
-constexpr int kSlots = 64;
-struct Plan {
-  Group g;
-  Layout L;
-  const DevTables *t = nullptr;
-  char *arena = nullptr;
-  DevBatch b;
-  cudaStream_t stream = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaEvent_t ev[kSlots][4] = {};
-  int launches = 0;
-  int device = 0;
-};
-
-void plan_free(Plan *p) {
-  if (!p) return;
-  if (p->stream) cudaStreamSynchronize(p->stream);
-  if (p->exec) cudaGraphExecDestroy(p->exec);
-  if (p->graph) cudaGraphDestroy(p->graph);
-  for (int s = 0; s < kSlots; s++)
-    for (int q = 0; q < 4; q++)
-      if (p->ev[s][q]) cudaEventDestroy(p->ev[s][q]);
-  if (p->arena) cudaFree(p->arena);
-  if (p->stream) cudaStreamDestroy(p->stream);
-  delete p;
-}
-}  // namespace
-
-mm_plan mm_plan_create(mm_context ctx, const MMFrontEndParams *params, const int64_t *lengths,
-                       int32_t n_clips, int32_t *status) {
-  int dummy;
-  int32_t *st_out = status ? status : &dummy;
-  *st_out = MM_ERR_INVALID_INPUT;
-  if (!ctx || !lengths || n_clips <= 0) return nullptr;
-  for (int i = 0; i < n_clips; i++)
-    if (lengths[i] <= 0) return nullptr;
-  Plan *p = new (std::nothrow) Plan();
-  if (!p) {
-    *st_out = MM_ERR_ALLOC_FAILED;
-    return nullptr;
-  }
-  int st = resolve_frontend(params, p->g);
-  if (st == MM_OK) st = gpu_available();
-  if (st == MM_OK) p->t = get_tables(p->g, &st);
-  if (st != MM_OK) {
-    *st_out = st;
-    delete p;
-    return nullptr;
-  }
-  cudaGetDevice(&p->device);
-  p->g.variant = group_variant(p->g);
-  make_layout(p->g, lengths, n_clips, p->L);
-  cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaMalloc(&p->arena, arena_bytes(p->g, p->L));
-  if (e == cudaSuccess) {
-    const size_t desc = carve_arena(p->g, p->L, p->arena, p->b);
-    std::vector<char> host(desc + 16);
-    pack_descriptors(p->L, host.data());
-    e = cudaMemsetAsync(p->arena, 0, sizeof(float) * (size_t)p->L.sig_elems, p->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(p->b.clips, host.data(), desc, cudaMemcpyHostToDevice, p->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
-  }
-  for (int s = 0; s < kSlots && e == cudaSuccess; s++)
-    for (int q = 0; q < 4 && e == cudaSuccess; q++) e = cudaEventCreate(&p->ev[s][q]);
-  if (e == cudaSuccess) e = cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeRelaxed);
-  if (e == cudaSuccess) {
-    cudaError_t e1 = enqueue_batch(p->g, p->L, p->t, p->b, p->stream, nullptr, &p->launches);
-    cudaError_t e2 = cudaStreamEndCapture(p->stream, &p->graph);
-    e = (e1 != cudaSuccess) ? e1 : e2;
-  }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec, p->graph, 0);
-  if (e != cudaSuccess) {
-    cudaGetLastError();
-    *st_out = cuda_status(e);
-    plan_free(p);
-    return nullptr;
-  }
-  *st_out = MM_OK;
-  return p;
-}
-
-void mm_plan_destroy(mm_plan plan) { plan_free(static_cast<Plan *>(plan)); }
-
-float *mm_plan_device_input(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.signal : nullptr; }
-float *mm_plan_device_output(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.out : nullptr; }
-
-int64_t mm_plan_input_offset(mm_plan plan, int32_t clip) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
-  return p->L.clips[clip].sig_off;
-}
-int64_t mm_plan_output_offset(mm_plan plan, int32_t clip) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
-  return p->L.clips[clip].out_off;
-}
-int64_t mm_plan_clip_frames(mm_plan plan, int32_t clip) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || clip < 0 || clip >= (int)p->L.clips.size()) return -1;
-  return p->L.clips[clip].n_frames;
-}
-int32_t mm_plan_rows(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->g.n_mfcc_eff : -1; }
-int64_t mm_plan_total_frames(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->L.total_frames : -1; }
-int32_t mm_plan_kernel_launches(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->launches : -1; }
-
-float *mm_plan_device_mel_db(mm_plan plan) { return plan ? static_cast<Plan *>(plan)->b.meldb : nullptr; }
-
-int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float *max_db) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || clip < 0 || clip >= (int)p->L.clips.size() || !max_db) return MM_ERR_INVALID_INPUT;
-  unsigned u = 0;
-  cudaError_t e = cudaMemcpy(&u, p->b.clip_max + clip, sizeof(unsigned), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return cuda_status(e);
-  *max_db = decode_max(u);
-  return MM_OK;
-}
-
-int32_t mm_plan_execute(mm_plan plan, void *stream) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p) return MM_ERR_INVALID_INPUT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
-  return cuda_status(cudaGraphLaunch(p->exec, s));
-}
-
-int32_t mm_plan_execute_timed(mm_plan plan, void *stream, int32_t slot) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || slot < 0 || slot >= kSlots) return MM_ERR_INVALID_INPUT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
-  return cuda_status(enqueue_batch(p->g, p->L, p->t, p->b, s, p->ev[slot], nullptr));
-}
-
-int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float *ms3) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || slot < 0 || slot >= kSlots || !ms3) return MM_ERR_INVALID_INPUT;
-  for (int q = 0; q < 3; q++) {
-    cudaError_t e = cudaEventElapsedTime(&ms3[q], p->ev[slot][q], p->ev[slot][q + 1]);
-    if (e != cudaSuccess) return cuda_status(e);
-  }
-  return MM_OK;
-}
-
-int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *const *outs, void *stream) {
-  Plan *p = static_cast<Plan *>(plan);
-  if (!p || !signals || !outs) return MM_ERR_INVALID_INPUT;
-  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
-  cudaError_t e = cudaSuccess;
-  const int n = (int)p->L.clips.size();
-  for (int i = 0; i < n && e == cudaSuccess; i++) {
-    const ClipDesc &c = p->L.clips[i];
-    e = cudaMemcpyAsync(p->b.signal + c.sig_off, signals[i], sizeof(float) * (size_t)c.length,
-                        cudaMemcpyHostToDevice, s);
-  }
-  if (e == cudaSuccess) e = cudaGraphLaunch(p->exec, s);
-  const int rows = p->g.n_mfcc_eff;
-  for (int i = 0; i < n && e == cudaSuccess; i++) {
-    const ClipDesc &c = p->L.clips[i];
-    const size_t cnt = (size_t)rows * (size_t)c.n_frames;
-    if (cnt) e = cudaMemcpyAsync(outs[i], p->b.out + c.out_off, sizeof(float) * cnt, cudaMemcpyDeviceToHost, s);
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  return cuda_status(e);
-}
-
 int32_t mm_tune_set(int32_t n_fft, int32_t variant) {
   if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 || variant > kWarpVariant) return MM_ERR_INVALID_INPUT;
   set_tuned_variant(ilog2(n_fft), variant);

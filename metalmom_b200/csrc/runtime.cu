@@ -60,6 +60,13 @@ long long frame_count(long long length, int n_fft, int hop, int center) {
   return 1 + (padded - n_fft) / hop;
 }
 
+bool same_group(const Group &a, const Group &b) {
+  return std::tie(a.mode, a.sr, a.n_fft, a.hop, a.win, a.window_zero, a.center, a.pad_mode, a.n_mels,
+                  a.n_mfcc_eff, a.fmin, a.fmax, a.top_db, a.power, a.amin, a.ref) ==
+         std::tie(b.mode, b.sr, b.n_fft, b.hop, b.win, b.window_zero, b.center, b.pad_mode, b.n_mels,
+                  b.n_mfcc_eff, b.fmin, b.fmax, b.top_db, b.power, b.amin, b.ref);
+}
+
 int output_rows(const Group &g) {
   switch (g.mode) {
     case MODE_SPECTRUM: return g.n_fft / 2 + 1;

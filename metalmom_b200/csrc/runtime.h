@@ -41,6 +41,9 @@ long long frame_count(long long length, int n_fft, int hop, int center);
 // Rows of one clip's output block for the group's mode.
 int output_rows(const Group &g);
 
+// True when two groups launch identically (clips of both can share a batch).
+bool same_group(const Group &a, const Group &b);
+
 // MFCC-path group from MMFrontEndParams (sentinels of mm_mfcc, pad mode,
 // top_db); MM_ERR_INVALID_INPUT for unsupported values.
 int resolve_frontend(const MMFrontEndParams *p, Group &g);

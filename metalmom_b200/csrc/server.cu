@@ -122,13 +122,6 @@ struct Request {
   Clock::time_point t_submit, t_done;
 };
 
-// Requests batch together when every launch parameter agrees.
-bool same_group(const Group &a, const Group &b) {
-  return std::tie(a.sr, a.n_fft, a.hop, a.win, a.center, a.pad_mode, a.n_mels, a.n_mfcc_eff, a.fmin, a.fmax,
-                  a.top_db) == std::tie(b.sr, b.n_fft, b.hop, b.win, b.center, b.pad_mode, b.n_mels,
-                                        b.n_mfcc_eff, b.fmin, b.fmax, b.top_db);
-}
-
 struct Server;
 
 struct Slot {

@@ -117,3 +117,5 @@ def test_no_gpu_is_reported_not_hidden():
         M.Plan([4096, 5000])
     with pytest.raises(RuntimeError, match="status -2"):
         M.Server()
+    with pytest.raises(RuntimeError, match="status -2"):
+        M.Plan([4096, 5000], clip_params=[dict(sr=22050), dict(sr=16000, n_fft=512)])

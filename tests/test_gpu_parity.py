@@ -272,6 +272,70 @@ def test_plan_graph_replay_and_host_io():
             np.testing.assert_array_equal(x, r)
 
 
+def _uneven_group(rng):
+    """A parameter group of the uneven-batch workload: sr 22050/44100, n_fft
+    1024/2048/4096 with hop n_fft/4, 64/128 mels, 20 MFCC."""
+    n_fft = int(rng.choice([1024, 2048, 4096]))
+    return dict(sr=int(rng.choice([22050, 44100])), n_fft=n_fft, hop_length=n_fft // 4,
+                n_mels=int(rng.choice([64, 128])), n_mfcc=20)
+
+
+@pytest.mark.parametrize("max_per_branch", [0, 4])
+def test_grouped_plan_uneven_mixed_groups(max_per_branch):
+    """Clips with their own parameter groups in one graph: equal to per-clip
+    calls (bitwise) through host I/O and through graph replay."""
+    rng = np.random.default_rng(40 + max_per_branch)
+    params, clips = [], []
+    for i in range(30):
+        g = _uneven_group(rng) if i % 5 else dict(sr=16000, n_fft=512, hop_length=160, win_length=400,
+                                                    n_mels=80, n_mfcc=13, fmin=20.0, fmax=8000.0)
+        L = int(rng.integers(1, 4 * g["sr"]))
+        params.append(g)
+        clips.append((synth.speech_clip if g["sr"] == 16000 else synth.music_clip)(L, g["sr"], seed=500 + i))
+    with M.Plan([len(c) for c in clips], clip_params=params, max_clips_per_branch=max_per_branch) as plan:
+        n_groups = len({tuple(sorted(g.items())) for g in params})
+        assert plan.branches >= n_groups
+        if max_per_branch:
+            assert plan.branches > n_groups
+        outs = plan.execute_host(clips)
+        again = plan.execute_host(clips)
+        plan.execute()
+    for c, g, o, o2 in zip(clips, params, outs, again):
+        ref = M.mfcc_batch([c], **g)[0]
+        assert o.shape == ref.shape
+        np.testing.assert_array_equal(o, ref)
+        np.testing.assert_array_equal(o2, ref)
+    for c, g, o in list(zip(clips, params, outs))[:6]:
+        exp = O.mfcc(c, g["sr"], g["n_mfcc"], g["n_fft"], g["hop_length"], g.get("win_length", g["n_fft"]),
+                     g["n_mels"], g.get("fmin", 0.0), g.get("fmax"))
+        if exp.size:
+            assert O.mfcc_rel_error(o, exp) < MFCC_TOL
+
+
+def test_grouped_plan_graph_replay_on_device_inputs():
+    import torch
+    rng = np.random.default_rng(77)
+    params = [_uneven_group(rng) for _ in range(12)]
+    clips = [synth.music_clip(int(rng.integers(3000, 3 * g["sr"])), g["sr"], seed=900 + i)
+             for i, g in enumerate(params)]
+    with M.Plan([len(c) for c in clips], clip_params=params, max_clips_per_branch=3) as plan:
+        base = plan.device_input
+        for c, off in zip(clips, plan.in_offsets):
+            dst = torch.as_tensor(_DevFloats(base + 4 * off, len(c)), device="cuda")
+            dst.copy_(torch.from_numpy(c).cuda())
+        torch.cuda.synchronize()
+        plan.execute()
+        torch.cuda.synchronize()
+        for c, g, off, r, f in zip(clips, params, plan.out_offsets, plan.clip_rows, plan.frames):
+            got = torch.as_tensor(_DevFloats(plan.device_output + 4 * off, r * f), device="cuda").cpu().numpy()
+            np.testing.assert_array_equal(got.reshape(r, f), M.mfcc_batch([c], **g)[0])
+
+
+class _DevFloats:
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (ptr, False), "version": 2}
+
+
 # ---------------------------------------------------------------------------
 # launch variants (autotuner search space): every variant is parity-checked
 # ---------------------------------------------------------------------------

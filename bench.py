@@ -289,6 +289,54 @@ def serving_leg(duration=3.0, rates=(50, 500, 2000), burst=2000, plain_s=2.0):
     return res
 
 
+def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
+    """The uneven batch: 1024 clips, lengths uniform in 1-120 s, each clip
+    with its own group (sr 22050/44100, n_fft 1024/2048/4096 with hop n_fft/4,
+    64/128 mels, 20 MFCC); launch variants autotuned per n_fft; one grouped
+    plan (a graph of concurrent persistent launches, one branch per group),
+    inputs resident, CUDA events around `steps` graph replays."""
+    import torch
+    import metalmom_b200 as M
+    from metalmom_b200 import synth
+    rng = np.random.default_rng(seed)
+    pools = {sr: synth.music_clip(120 * sr, sr, seed=sr) for sr in (22050, 44100)}
+    params, clips = [], []
+    for _ in range(n_clips):
+        n_fft = int(rng.choice([1024, 2048, 4096]))
+        g = dict(sr=int(rng.choice([22050, 44100])), n_fft=n_fft, hop_length=n_fft // 4,
+                 n_mels=int(rng.choice([64, 128])), n_mfcc=20)
+        n = int(rng.uniform(1.0, 120.0) * g["sr"])
+        start = int(rng.integers(0, len(pools[g["sr"]]) - n + 1))
+        params.append(g)
+        clips.append(pools[g["sr"]][start:start + n])
+    tuned = {}
+    for n_fft in (1024, 2048, 4096):
+        tuned[n_fft] = M.autotune(clip_samples=30 * 22050, n_clips=32, reps=3, sr=22050, n_fft=n_fft,
+                                  hop_length=n_fft // 4, n_mels=128, n_mfcc=20)["best"]
+    plan = M.Plan([len(c) for c in clips], clip_params=params)
+    sh = stream.cuda_stream
+    plan.execute_host(clips, stream=sh)
+    for _ in range(3):
+        plan.execute(stream=sh)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        plan.execute(stream=sh)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    hours = sum(len(c) / g["sr"] for c, g in zip(clips, params)) / 3600.0
+    out = {"workload": f"{n_clips} clips, lengths U[1,120] s, per-clip group from sr {{22050, 44100}} x "
+                       "n_fft {1024, 2048, 4096} (hop n_fft/4) x mels {64, 128}, 20 MFCC",
+           "audio_hours": hours, "ms_per_step": ms, "audio_hours_per_s": hours / (ms / 1e3),
+           "groups": len({tuple(sorted(g.items())) for g in params}), "branches": plan.branches,
+           "gpu_launches_per_step": plan.kernel_launches, "tuned_variant_per_n_fft": tuned,
+           "timing": "CUDA events around graph replays, inputs resident (> L2)"}
+    plan.close()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import metalmom_b200 as M
@@ -314,11 +362,15 @@ def run_ours(args, rank, world, local_rank):
     sh = stream.cuda_stream
     assert sh != 0
 
-    # pinned host buffers for the end-to-end leg
+    # pinned host buffers for the end-to-end leg, which runs through a plan cut
+    # into branches so that one branch's copies overlap another's kernels
     pin_in = [torch.from_numpy(c).pin_memory() for c in clips]
     in_np = [t.numpy() for t in pin_in]
     pin_out = [torch.empty((plan.rows, f), dtype=torch.float32).pin_memory() for f in plan.frames]
     out_np = [t.numpy() for t in pin_out]
+    plan_io = M.Plan(lengths, clip_params=[dict(sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS,
+                                                n_mfcc=N_MFCC)] * n_clips,
+                     max_clips_per_branch=args.e2e_branch_clips)
     plan.execute_host(in_np, out_np, stream=sh)  # uploads the inputs once
     torch.cuda.synchronize()
 
@@ -353,14 +405,14 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- end-to-end through the public API (pinned host in/out every step)
     for _ in range(max(1, W // 2)):
-        plan.execute_host(in_np, out_np, stream=sh)
+        plan_io.execute_host(in_np, out_np, stream=sh)
     torch.cuda.synchronize()
     barrier()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ke = max(1, min(K, args.e2e_steps))
     e_start.record(stream)
     for _ in range(ke):
-        plan.execute_host(in_np, out_np, stream=sh)
+        plan_io.execute_host(in_np, out_np, stream=sh)
     e_end.record(stream)
     torch.cuda.synchronize()
     e_ms = e_start.elapsed_time(e_end)
@@ -440,8 +492,8 @@ def run_ours(args, rank, world, local_rank):
                          "pipeline_frac": pipe_bytes / (ms_step / 1e3) / 1e9 / hbm,
                          "fp32_fft_tflops": flops_fft / (frame_ms / 1e3) / 1e12},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": ke,
-                    "api": "Plan.execute_host (mm_plan_execute_host)"},
+                    "d2h_bytes_per_step": d2h, "steps": ke, "branches": plan_io.branches,
+                    "api": "Plan.execute_host (mm_plan_execute_host), pinned host buffers"},
             "clocks": clk.summary(),
             "gpu_launches": K * plan.kernel_launches,
             "one_clip_per_launch": per_clip,
@@ -454,7 +506,10 @@ def run_ours(args, rank, world, local_rank):
             result.update(baseline_leg(plan, clips, world, args))
         if not args.no_serve:
             result["serving"] = serving_leg()
+        if not args.no_uneven:
+            result["uneven_batch"] = uneven_leg(stream)
     plan.close()
+    plan_io.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -505,6 +560,8 @@ def main():
     ap.add_argument("--ref-clips", type=int, default=32)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--e2e-branch-clips", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))

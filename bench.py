@@ -337,6 +337,59 @@ def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
     return out
 
 
+def precision_leg(stream, n_clips=512, steps=10):
+    """The speech front end (16 kHz, n_fft 512, win 400, hop 160, 80 mels
+    20-8000 Hz, 13 MFCC) on 512 clips x 10 s in three DFT forms: the float32
+    FFT, the DFT as a tcgen05 GEMM with bf16x3 split products (float32
+    accumulation) and with plain bf16; device-resident throughput of each
+    (graph replays, CUDA events) and max/mean mel-dB and MFCC error against the
+    FP64 oracle on 4 clips."""
+    import torch
+    import metalmom_b200 as M
+    from metalmom_b200 import synth
+    from oracle import oracle as O
+    pool = synth.speech_clip(600 * 16000, 16000, seed=2025)
+    rng = np.random.default_rng(7)
+    L = 160000
+    starts = rng.integers(0, len(pool) - L, n_clips)
+    clips = [pool[s:s + L] for s in starts]
+    M.autotune(clip_samples=L, n_clips=32, reps=3, **SERVE_SPEECH)
+    sh = stream.cuda_stream
+    check = [0, 1, n_clips // 2, n_clips - 1]
+    exp_db = [O.mel_db(clips[i], 16000, 512, 160, 400, True, 80, 20.0, 8000.0) for i in check]
+    exp_c = [O.mfcc(clips[i], 16000, 13, 512, 160, 400, 80, 20.0, 8000.0) for i in check]
+    out = {"workload": f"{n_clips} clips x 10 s @16 kHz speech-like, n_fft 512, win 400, hop 160, 80 mels, 13 MFCC",
+           "forms": {}}
+    hours = n_clips * L / 16000 / 3600.0
+    for form in ("fft", "bf16x3", "bf16"):
+        with M.Plan([L] * n_clips, dft=form, **SERVE_SPEECH) as plan:
+            res = plan.execute_host(clips, stream=sh)
+            for _ in range(3):
+                plan.execute(stream=sh)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(steps):
+                plan.execute(stream=sh)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms = a.elapsed_time(b) / steps
+            frame0 = np.concatenate([[0], np.cumsum(plan.frames)])
+            db_max, db_mean, c_max = 0.0, [], 0.0
+            for j, i in enumerate(check):
+                T = plan.frames[i]
+                mel = _device_floats(plan.device_mel_db + 4 * int(frame0[i]) * 80, T * 80)
+                mel = np.maximum(mel.reshape(T, 80).T.astype(np.float64), plan.clip_max_db(i) - 80.0)
+                d = np.abs(mel - exp_db[j])
+                db_max = max(db_max, float(d.max()))
+                db_mean.append(float(d.mean()))
+                c_max = max(c_max, O.mfcc_rel_error(res[i], exp_c[j]))
+        out["forms"][form] = {"audio_hours_per_s": hours / (ms / 1e3), "ms_per_step": ms,
+                              "mel_db_max_abs_err_db": db_max, "mel_db_mean_abs_err_db": float(np.mean(db_mean)),
+                              "mfcc_max_err_rel_to_max": c_max}
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import metalmom_b200 as M
@@ -508,6 +561,8 @@ def run_ours(args, rank, world, local_rank):
             result["serving"] = serving_leg()
         if not args.no_uneven:
             result["uneven_batch"] = uneven_leg(stream)
+        if not args.no_precision:
+            result["precision_forms"] = precision_leg(stream)
     plan.close()
     plan_io.close()
     if dist is not None:
@@ -561,6 +616,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--e2e-branch-clips", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

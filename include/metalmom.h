@@ -107,6 +107,14 @@ MM_API void mm_buffer_free(MMBuffer* buf);
 #define MM_PAD_CONSTANT 0 /* zeros: the reference's centering */
 #define MM_PAD_REFLECT 1  /* mirror without repeating the edge sample */
 
+/* How the spectrum is computed: the float32 FFT (default), or the DFT as a
+ * GEMM on the tensor cores (n_fft 256..1024, window <= n_fft) with bf16
+ * operands split in two parts (three products, float32 accumulation) or
+ * plain bf16.  The GEMM forms exist for the precision comparison. */
+#define MM_DFT_FFT_F32 0
+#define MM_DFT_GEMM_BF16X3 1
+#define MM_DFT_GEMM_BF16 2
+
 /* One front-end parameter group.  Sentinels as in mm_mfcc. */
 typedef struct {
     int32_t sample_rate;
@@ -120,7 +128,7 @@ typedef struct {
     float f_min;
     float f_max;        /* <= 0: sr/2 */
     float top_db;       /* <= 0: no floor; mm_mfcc uses 80 */
-    int32_t reserved;
+    int32_t dft_form;   /* MM_DFT_FFT_F32 (0), MM_DFT_GEMM_BF16X3 or MM_DFT_GEMM_BF16 */
 } MMFrontEndParams;
 
 /* MFCC of n_clips clips of any lengths in one batched launch sequence.

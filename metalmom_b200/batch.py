@@ -14,7 +14,7 @@ from ._native import ffi, lib
 
 def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, center=True,
                     pad_mode="constant", n_mels=128, n_mfcc=20, fmin=0.0, fmax=None,
-                    top_db=80.0):
+                    top_db=80.0, dft="fft"):
     """An ``MMFrontEndParams`` struct (sentinels: None -> reference defaults)."""
     p = ffi.new("MMFrontEndParams*")
     p.sample_rate = sr
@@ -28,6 +28,8 @@ def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, cent
     p.f_min = fmin
     p.f_max = float(fmax) if fmax is not None else 0.0
     p.top_db = float(top_db) if top_db is not None else 0.0
+    p.dft_form = {"fft": lib.MM_DFT_FFT_F32, "bf16x3": lib.MM_DFT_GEMM_BF16X3,
+                  "bf16": lib.MM_DFT_GEMM_BF16}[dft]
     return p
 
 

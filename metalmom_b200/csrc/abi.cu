@@ -64,6 +64,15 @@ int run_batch(const Group &g_in, const float *const *signals, const int64_t *len
   if ((e = cudaMemcpyAsync(h, b.out, out_bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_status(e);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e);
+  if (t->dft_err) {  // a bounded wait of the tensor-core kernel ran out
+    unsigned flag = 0;
+    if ((e = cudaMemcpy(&flag, t->dft_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess)
+      return cuda_status(e);
+    if (flag) {
+      cudaMemset(t->dft_err, 0, sizeof(unsigned));
+      return MM_ERR_INTERNAL;
+    }
+  }
   const int rows = output_rows(g);
   for (int i = 0; i < n; i++) {
     const size_t cnt = (size_t)rows * (size_t)L.clips[i].n_frames;
@@ -264,6 +273,9 @@ int mm::resolve_frontend(const MMFrontEndParams *p, Group &g) {
   if (p->n_mfcc < 0 || (p->pad_mode != MM_PAD_CONSTANT && p->pad_mode != MM_PAD_REFLECT))
     return MM_ERR_INVALID_INPUT;
   if (!is_pow2(p->n_fft) || !supported_size(g)) return MM_ERR_INVALID_INPUT;
+  if (p->dft_form < MM_DFT_FFT_F32 || p->dft_form > MM_DFT_GEMM_BF16) return MM_ERR_INVALID_INPUT;
+  if (p->dft_form != MM_DFT_FFT_F32 && !dft_supported(g.n_fft, g.win)) return MM_ERR_INVALID_INPUT;
+  g.dft_form = p->dft_form;
   g.mode = MODE_MELDB;
   g.pad_mode = p->pad_mode;
   g.power = 2.0f;

@@ -150,6 +150,7 @@ static int frames_for(int v) {
 }
 
 int frames_per_tile(int log2n, int variant) {
+  if (variant == kDftVariant) return 128;
   if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0) return warp_frames_per_tile(log2n);
   switch (log2n) {
     case 5: return frames_for<5>(variant);

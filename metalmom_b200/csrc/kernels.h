@@ -1,6 +1,7 @@
 // Interfaces between the host runtime (mm_runtime.cpp / mm_abi.cpp) and the
 // CUDA kernels (frontend_kernels.cu).  Plain structs and pointers only.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -24,6 +25,15 @@ enum FrontMode : int {
 
 enum PadMode : int { PAD_CONSTANT = 0, PAD_REFLECT = 1 };
 
+// How the spectrum is computed (MMFrontEndParams.dft_form).
+enum DftForm : int { DFT_FFT_F32 = 0, DFT_GEMM_BF16X3 = 1, DFT_GEMM_BF16 = 2 };
+
+// Geometry of the DFT-as-GEMM form: bins, N tiles of tile_cols columns
+// (cos / -sin per bin), the window support [k0, k0 + kw) cut into K chunks.
+struct DftShape {
+  int n_fft, nbins, ntiles, tile_cols, k0, kw, kchunks;
+};
+
 // Device tables for one (sr, n_fft, win, n_mels, fmin, fmax, n_mfcc) group.
 struct DevTables {
   int n_fft = 0, n_mels = 0, n_mfcc = 0;
@@ -42,6 +52,11 @@ struct DevTables {
   float2 *mel_w2 = nullptr;
   int2 *mel_seg = nullptr;
   int mel_seg_ok = 0;          // 0: the split does not describe the filterbank (use mel_pw)
+  // DFT-as-GEMM form only: the windowed DFT basis as bf16 hi/lo images and an
+  // error word the kernel sets when a bounded wait runs out.
+  __nv_bfloat16 *dft_basis = nullptr;
+  DftShape dft{};
+  unsigned *dft_err = nullptr;
   float *dct = nullptr;        // [n_mfcc_eff][n_mels] DCT-II ortho basis
 };
 
@@ -108,6 +123,15 @@ cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, 
 
 // Blocks per SM and SM count for a persistent launch of `kern` (cached).
 cudaError_t persistent_geometry(const void *kern, int threads, size_t smem, int *per_sm, int *sms);
+
+// DFT-as-GEMM (tcgen05) form: n_fft 256..1024, window no longer than n_fft.
+constexpr int kDftVariant = 4;  // launch "variant" of such groups (128-frame tiles)
+bool dft_supported(int n_fft, int win);
+DftShape dft_shape(int n_fft, int win);
+size_t dft_basis_bytes(const DftShape &s);
+cudaError_t build_dft_basis(__nv_bfloat16 *img, const DftShape &s, int win, int window_zero, cudaStream_t st);
+cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, const __nv_bfloat16 *basis,
+                            unsigned *err, cudaStream_t st, int *launched);
 
 // Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
 cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,

@@ -42,6 +42,7 @@ void set_tuned_variant(int log2n, int v) {
   if (log2n >= 0 && log2n < 16) g_tuned[log2n].store(v);
 }
 int group_variant(const Group &g) {
+  if (g.dft_form != DFT_FFT_F32) return kDftVariant;
   const int nv = frame_variants(g.log2n, g.mode, g.power == 2.0f);
   const int v = tuned_variant(g.log2n);
   return (v >= 0 && v < nv) ? v : 0;
@@ -62,9 +63,9 @@ long long frame_count(long long length, int n_fft, int hop, int center) {
 
 bool same_group(const Group &a, const Group &b) {
   return std::tie(a.mode, a.sr, a.n_fft, a.hop, a.win, a.window_zero, a.center, a.pad_mode, a.n_mels,
-                  a.n_mfcc_eff, a.fmin, a.fmax, a.top_db, a.power, a.amin, a.ref) ==
+                  a.n_mfcc_eff, a.fmin, a.fmax, a.top_db, a.power, a.amin, a.ref, a.dft_form) ==
          std::tie(b.mode, b.sr, b.n_fft, b.hop, b.win, b.window_zero, b.center, b.pad_mode, b.n_mels,
-                  b.n_mfcc_eff, b.fmin, b.fmax, b.top_db, b.power, b.amin, b.ref);
+                  b.n_mfcc_eff, b.fmin, b.fmax, b.top_db, b.power, b.amin, b.ref, b.dft_form);
 }
 
 int output_rows(const Group &g) {
@@ -82,9 +83,10 @@ namespace {
 struct TableKey {
   int dev, sr, n_fft, win, window_zero, n_mels, n_mfcc;
   float fmin, fmax;
+  int dft;  // 1: also the DFT-as-GEMM basis
   bool operator<(const TableKey &o) const {
-    return std::tie(dev, sr, n_fft, win, window_zero, n_mels, n_mfcc, fmin, fmax) <
-           std::tie(o.dev, o.sr, o.n_fft, o.win, o.window_zero, o.n_mels, o.n_mfcc, o.fmin, o.fmax);
+    return std::tie(dev, sr, n_fft, win, window_zero, n_mels, n_mfcc, fmin, fmax, dft) <
+           std::tie(o.dev, o.sr, o.n_fft, o.win, o.window_zero, o.n_mels, o.n_mfcc, o.fmin, o.fmax, o.dft);
   }
 };
 std::mutex g_table_mu;
@@ -100,7 +102,7 @@ const DevTables *get_tables(const Group &g, int *status) {
   }
   const int n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
   const int n_mfcc = (g.mode == MODE_MELDB) ? g.n_mfcc_eff : 0;
-  TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax};
+  TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax, g.dft_form != 0 ? 1 : 0};
   std::lock_guard<std::mutex> lock(g_table_mu);
   auto it = g_tables.find(k);
   if (it != g_tables.end()) {
@@ -112,6 +114,13 @@ const DevTables *get_tables(const Group &g, int *status) {
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e == cudaSuccess) {
     e = build_tables(*t, g.sr, g.n_fft, g.win, n_mels, g.fmin, g.fmax, n_mfcc, g.window_zero, s);
+    if (e == cudaSuccess && g.dft_form != DFT_FFT_F32) {
+      t->dft = dft_shape(g.n_fft, g.win);
+      e = cudaMalloc(&t->dft_basis, dft_basis_bytes(t->dft));
+      if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
+      if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
+      if (e == cudaSuccess) e = build_dft_basis(t->dft_basis, t->dft, g.win, g.window_zero, s);
+    }
     cudaError_t e2 = cudaStreamSynchronize(s);
     if (e == cudaSuccess) e = e2;
     cudaStreamDestroy(s);
@@ -128,6 +137,8 @@ const DevTables *get_tables(const Group &g, int *status) {
     cudaFree(t->mel_w2);
     cudaFree(t->mel_seg);
     cudaFree(t->dct);
+    cudaFree(t->dft_basis);
+    cudaFree(t->dft_err);
     delete t;
     return nullptr;
   }
@@ -271,7 +282,11 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.out = (g.mode == MODE_MELDB) ? b.meldb : b.out;
   a.clip_max = b.clip_max;
   int grid = 0;
-  if ((e = launch_frontend(g.log2n, g.mode, g.variant, a, 0, s, &grid)) != cudaSuccess) return e;
+  if (g.dft_form != DFT_FFT_F32 && g.mode == MODE_MELDB)
+    e = launch_dft_gemm(g.dft_form, a, t->dft, t->dft_basis, t->dft_err, s, &grid);
+  else
+    e = launch_frontend(g.log2n, g.mode, g.variant, a, 0, s, &grid);
+  if (e != cudaSuccess) return e;
   if (grid > 0) launches++;
   if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
   if (g.mode == MODE_MELDB && g.n_mfcc_eff > 0 && !L.dct_tile_clip.empty()) {

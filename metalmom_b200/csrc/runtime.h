@@ -25,6 +25,7 @@ struct Group {
   float fmin = 0.0f, fmax = 11025.0f, top_db = 80.0f;
   float power = 2.0f, amin = 1e-10f, ref = 1.0f;
   int variant = 0;  // frame-kernel launch variant (autotuned per n_fft)
+  int dft_form = DFT_FFT_F32;
 };
 
 // Process-wide autotuning table: launch variant per log2(n_fft).

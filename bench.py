@@ -405,8 +405,12 @@ def run_ours(args, rank, world, local_rank):
     n_clips = args.clips
     clips = make_clips(n_clips, seed0=1000 * rank)
     lengths = [len(c) for c in clips]
-    tune = M.autotune(clip_samples=CLIP_SAMPLES, n_clips=min(n_clips, 64), reps=5, sr=SR,
-                      n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
+    if args.variant is None:
+        tune = M.autotune(clip_samples=CLIP_SAMPLES, n_clips=min(n_clips, 64), reps=5, sr=SR,
+                          n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
+    else:  # a fixed launch variant (profiling runs, where the tuner's timings are distorted)
+        M.tune_set(N_FFT, args.variant)
+        tune = {"best": args.variant, "ms": []}
     plan = M.Plan(lengths, sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS, n_mfcc=N_MFCC)
     # an explicit stream: handle 0 (the legacy default stream) would mean "the
     # plan's own stream" to the C ABI, outside these events
@@ -617,6 +621,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--variant", type=int, default=None, help="fixed frame-kernel launch variant (no autotuning)")
     ap.add_argument("--e2e-branch-clips", type=int, default=32)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

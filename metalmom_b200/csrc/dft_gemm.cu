@@ -39,7 +39,7 @@ namespace mm {
 
 constexpr int kDftM = 128;   // frames per tile = TMEM lanes
 constexpr int kDftKC = 64;   // K per chunk: one 128-byte swizzle row of bf16
-constexpr int kDftThreads = 128;
+constexpr int kDftThreads = 256;  // 8 warps: two per TMEM lane quarter
 constexpr int kDftTmemCols = 256;
 constexpr size_t kDftMinSmem = 80 * 1024;  // at most two CTAs per SM: 2 x 256 TMEM columns
 
@@ -202,32 +202,73 @@ __device__ __forceinline__ void split8(const float *x, uint4 &hi, uint4 &lo) {
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+constexpr int kDftStages = 2;
+
+// 32 samples (x[first + q], q < 32) of one frame row, with the padding rule
+// of sample_at; zeros for frames past the clip.
+__device__ __forceinline__ void load_row32(float *x, const float *sig, long long first, long long length,
+                                           long long sig_off, int pad_mode, bool valid) {
+  if (valid && first >= 0 && first + 32 <= length && ((sig_off + first) & 3) == 0) {
+    const float4 *p4 = reinterpret_cast<const float4 *>(sig + first);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const float4 v = __ldg(p4 + q);
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < 32; q++) x[q] = valid ? sample_at(sig, first + q, length, pad_mode) : 0.0f;
+  }
+}
+
 struct DftSmem {
-  size_t a_hi, a_lo, b_hi, b_lo, w2, seg, mbar, taddr, total;
+  size_t a_hi[kDftStages], a_lo[kDftStages], b_hi[kDftStages], b_lo[kDftStages];
+  size_t w2, seg, bar, taddr, total;
 };
 __host__ __device__ inline DftSmem dft_smem_layout(const DftShape &s, int n_mels) {
   DftSmem L{};
   size_t p = 0;
-  const size_t a_bytes = (size_t)kDftM * 128, b_bytes = (size_t)s.tile_cols * 128;
-  L.a_hi = p;
-  p += a_bytes;
-  L.a_lo = p;
-  p += a_bytes;
-  L.b_hi = p;
-  p += (b_bytes + 1023) & ~size_t(1023);
-  L.b_lo = p;
-  p += (b_bytes + 1023) & ~size_t(1023);
-  // the power spectrum of one N tile ([bins][128] floats) reuses A and B
+  const size_t a_bytes = (size_t)kDftM * 128, b_bytes = ((size_t)s.tile_cols * 128 + 1023) & ~size_t(1023);
+  for (int st = 0; st < kDftStages; st++) {
+    L.a_hi[st] = p;
+    p += a_bytes;
+    L.a_lo[st] = p;
+    p += a_bytes;
+    L.b_hi[st] = p;
+    p += b_bytes;
+    L.b_lo[st] = p;
+    p += b_bytes;
+  }
+  // the power spectrum of one N tile ([bins][128] floats) reuses the stages
   L.w2 = p;
   p += align16(8 * (size_t)s.nbins);
   L.seg = p;
   p += align16(8 * (size_t)(n_mels + 1));
-  L.mbar = p;
-  p += 16;
+  L.bar = p;  // full[2], empty[2]
+  p += 32;
   L.taddr = p;
   p += 16;
   L.total = p + 1024;  // slack to align the base to 1024 bytes
   return L;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+// One arrival that also announces `bytes` of bulk copies completing on the barrier.
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// 1-D bulk copy global -> shared (no multicast), completing on `bar`.
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
 }
 
 template <int SPLIT>
@@ -237,19 +278,25 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   const uint32_t raw = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const DftSmem Ly = dft_smem_layout(S, a.n_mels);
-  unsigned char *a_hi = sm + Ly.a_hi, *a_lo = sm + Ly.a_lo, *b_hi = sm + Ly.b_hi, *b_lo = sm + Ly.b_lo;
-  float *P = reinterpret_cast<float *>(sm);  // [bins of the tile][128], after the tile's MMAs
+  float *P = reinterpret_cast<float *>(sm);  // [bins of the N tile][128], after its MMAs
   float2 *w2_s = reinterpret_cast<float2 *>(sm + Ly.w2);
   int2 *seg_s = reinterpret_cast<int2 *>(sm + Ly.seg);
-  const uint32_t mbar = smem_u32(sm + Ly.mbar);
+  const uint32_t bar0 = smem_u32(sm + Ly.bar);
+  auto full_bar = [&](int st) { return bar0 + 8u * (uint32_t)st; };
+  auto empty_bar = [&](int st) { return bar0 + 16u + 8u * (uint32_t)st; };
   uint32_t *taddr_s = reinterpret_cast<uint32_t *>(sm + Ly.taddr);
 
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int row = tid & (kDftM - 1);  // frame of the tile (= TMEM lane)
+  const int half = tid >> 7;          // which 32 columns of a chunk this thread builds
   const int nmel = a.n_mels;
   for (int i = tid; i < S.nbins; i += kDftThreads) w2_s[i] = __ldg(a.mel_w2 + i);
   for (int i = tid; i <= nmel; i += kDftThreads) seg_s[i] = __ldg(a.mel_seg + i);
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar) : "memory");
+    for (int st = 0; st < kDftStages; st++) {
+      mbar_init(full_bar(st), 1);
+      mbar_init(empty_bar(st), 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -262,13 +309,17 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *taddr_s;
-  const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const uint32_t idesc = idesc_bf16(S.tile_cols);
-  const size_t b_img = (size_t)S.tile_cols * 128;
+  const uint32_t b_img = (uint32_t)S.tile_cols * 128u;
   const int seg_lo = seg_s[0].x, seg_hi = seg_s[nmel].x;
 
-  uint32_t phase = 0;
-  bool failed = false;
+  // per-stage state as bits (stage st = bit st): expected phase parities and
+  // whether an MMA commit on empty[st] has not been waited for yet
+  uint32_t full_ph = 0, empty_ph = 0, pend = 0;
+  const size_t stage_stride = Ly.a_hi[1] - Ly.a_hi[0];
+  uint32_t chunk = 0;
+  bool failed = false, broken = false;
   int cur_clip = -1;
   float vmax = -INFINITY;
   const int total = a.total_tiles;
@@ -286,12 +337,12 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
       vmax = -INFINITY;
     }
     const ClipDesc cd = load_clip(a.clips + c);
-    const int t = (tile - cd.tile_base) * kDftM + tid;  // this thread's frame
+    const int t = (tile - cd.tile_base) * kDftM + row;  // this thread's frame
     const bool valid = t < cd.n_frames;
     const float *sig = a.signal + cd.sig_off;
-    const long long s0 = (long long)t * a.hop - a.pad + S.k0;
+    const long long s0 = (long long)t * a.hop - a.pad + S.k0 + 32 * half;
     float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
-    // mel state (bins arrive in order across the N tiles)
+    // mel state of this frame (threads of half 0), bins arrive in order across N tiles
     int cur = 0;
     float Rprev = 0.0f, Rcur = 0.0f, Fcur = 0.0f, chk = 0.0f, fmax_ = -INFINITY;
     auto emit = [&](int m, float v) {
@@ -308,108 +359,134 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
       cur++;
     };
 
+    // samples of the next K chunk, loaded one chunk ahead (a chunk's samples
+    // are the same for every N tile)
+    float xn[32];
+    load_row32(xn, sig, s0, cd.length, cd.sig_off, a.pad_mode, valid);
     for (int nt = 0; nt < S.ntiles && !failed; nt++) {
       for (int kc = 0; kc < S.kchunks; kc++) {
-        // ---- A chunk: row tid = this frame's samples [s0 + 64 kc, +64)
+        const int st = (int)(chunk & 1u);
+        bool ok = true;
+        const uint32_t bit = 1u << st;
+        if (pend & bit) {  // the MMAs that read this stage two chunks ago are done
+          ok = mbar_wait_bounded(empty_bar(st), (empty_ph >> st) & 1u);
+          empty_ph ^= bit;
+          pend &= ~bit;
+        }
+        unsigned char *stage = sm + (size_t)st * stage_stride;
+        unsigned char *a_hi = stage + Ly.a_hi[0], *a_lo = stage + Ly.a_lo[0];
+        unsigned char *b_hi = stage + Ly.b_hi[0], *b_lo = stage + Ly.b_lo[0];
+        if (tid == 0 && ok && !broken) {
+          const char *src = reinterpret_cast<const char *>(basis) + (size_t)(nt * S.kchunks + kc) * 2 * b_img;
+          mbar_expect_tx(full_bar(st), SPLIT == 3 ? 2u * b_img : b_img);
+          bulk_g2s(smem_u32(b_hi), src, b_img, full_bar(st));
+          if (SPLIT == 3) bulk_g2s(smem_u32(b_lo), src + b_img, b_img, full_bar(st));
+        }
+        // ---- A chunk: this thread's 32 samples of its frame row
         {
-          const long long first = s0 + (long long)kc * kDftKC;
-          float x[kDftKC];
-          if (valid && first >= 0 && first + kDftKC <= cd.length && ((cd.sig_off + first) & 3) == 0) {
-            const float4 *p4 = reinterpret_cast<const float4 *>(sig + first);
+          float x[32];
 #pragma unroll
-            for (int q = 0; q < kDftKC / 4; q++) {
-              const float4 v = __ldg(p4 + q);
-              x[4 * q] = v.x;
-              x[4 * q + 1] = v.y;
-              x[4 * q + 2] = v.z;
-              x[4 * q + 3] = v.w;
-            }
-          } else {
-#pragma unroll
-            for (int q = 0; q < kDftKC; q++) x[q] = valid ? sample_at(sig, first + q, cd.length, a.pad_mode) : 0.0f;
+          for (int q = 0; q < 32; q++) x[q] = xn[q];
+          const bool last = kc + 1 == S.kchunks && nt + 1 == S.ntiles;
+          if (!last) {
+            const int kn = kc + 1 < S.kchunks ? kc + 1 : 0;
+            load_row32(xn, sig, s0 + (long long)kn * kDftKC, cd.length, cd.sig_off, a.pad_mode, valid);
           }
 #pragma unroll
-          for (int q = 0; q < 8; q++) {
+          for (int q = 0; q < 4; q++) {
             uint4 hi, lo;
             split8(x + 8 * q, hi, lo);
-            const uint32_t off = sw128(tid, 8 * q);
+            const uint32_t off = sw128(row, 32 * half + 8 * q);
             *reinterpret_cast<uint4 *>(a_hi + off) = hi;
             if (SPLIT == 3) *reinterpret_cast<uint4 *>(a_lo + off) = lo;
           }
         }
-        // ---- B chunk: copy the pre-swizzled image
-        {
-          const uint4 *src = reinterpret_cast<const uint4 *>(reinterpret_cast<const char *>(basis) +
-                                                             (size_t)(nt * S.kchunks + kc) * 2 * b_img);
-          const int n16 = (int)(b_img / 16);
-          for (int i = tid; i < n16; i += kDftThreads) {
-            reinterpret_cast<uint4 *>(b_hi)[i] = __ldg(src + i);
-            if (SPLIT == 3) reinterpret_cast<uint4 *>(b_lo)[i] = __ldg(src + n16 + i);
-          }
-        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
-          tc_fence_after();
-#pragma unroll
-          for (int kk = 0; kk < kDftKC / 16; kk++) {
-            const uint64_t dah = desc_sw128(smem_u32(a_hi) + kk * 32), dbh = desc_sw128(smem_u32(b_hi) + kk * 32);
-            umma_bf16(tmem, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
-            if (SPLIT == 3) {
-              const uint64_t dal = desc_sw128(smem_u32(a_lo) + kk * 32), dbl = desc_sw128(smem_u32(b_lo) + kk * 32);
-              umma_bf16(tmem, dah, dbl, idesc, 1u);
-              umma_bf16(tmem, dal, dbh, idesc, 1u);
-            }
-          }
-          umma_commit(mbar);
-        }
-        const bool ok = mbar_wait_bounded(mbar, phase);
-        if (__syncthreads_or(!ok)) {  // the same decision in every thread
+        if (__syncthreads_or(!ok)) {  // an MMA never completed: every thread decides alike
           failed = true;
           if (tid == 0) atomicOr(err, 1u);
           break;
         }
-        phase ^= 1u;
+        if (tid == 0 && !broken) {
+          if (mbar_wait_bounded(full_bar(st), (full_ph >> st) & 1u)) {
+            tc_fence_after();
+            const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
+            const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+#pragma unroll
+            for (int kk = 0; kk < kDftKC / 16; kk++) {
+              const uint64_t dah = desc_sw128(ah + kk * 32), dbh = desc_sw128(bh + kk * 32);
+              umma_bf16(tmem, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
+              if (SPLIT == 3) {
+                umma_bf16(tmem, dah, desc_sw128(bl + kk * 32), idesc, 1u);
+                umma_bf16(tmem, desc_sw128(al + kk * 32), dbh, idesc, 1u);
+              }
+            }
+            umma_commit(empty_bar(st));
+          } else {  // the basis never arrived: no commit, so the others time out on empty[st]
+            broken = true;
+            atomicOr(err, 1u);
+          }
+        }
+        full_ph ^= bit;
+        pend |= bit;
+        chunk++;
       }
       if (failed) break;
+      // ---- drain: the tile's accumulator is complete
+      bool ok = true;
+      for (int st = 0; st < kDftStages; st++)
+        if (pend & (1u << st)) {
+          ok = mbar_wait_bounded(empty_bar(st), (empty_ph >> st) & 1u) && ok;
+          empty_ph ^= 1u << st;
+          pend &= ~(1u << st);
+        }
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        if (tid == 0) atomicOr(err, 1u);
+        break;
+      }
       tc_fence_after();
-      // ---- accumulator -> |X|^2 of this tile's bins into P[bin][frame]
+      // ---- |X|^2 of this tile's bins into P[bin][frame]; the two warps of a
+      // lane quarter take alternate 16-column pieces
       const int kb = nt * S.tile_cols / 2;
       const int nb = min(S.tile_cols / 2, S.nbins - kb);
-      for (int col = 0; col < 2 * nb; col += 16) {
+      for (int col = 16 * half; col < 2 * nb; col += 32) {
         float v[16];
         tmem_ld16(lane_base + (uint32_t)col, v);
 #pragma unroll
         for (int b = 0; b < 8; b++) {
           const int bin = col / 2 + b;
-          if (bin < nb) {
-            const float p = fmaf(v[2 * b], v[2 * b], v[2 * b + 1] * v[2 * b + 1]);
-            P[bin * kDftM + tid] = p;
-            chk += p;
-          }
+          if (bin < nb) P[bin * kDftM + row] = fmaf(v[2 * b], v[2 * b], v[2 * b + 1] * v[2 * b + 1]);
         }
       }
-      // ---- fold this tile's bins into the mel bands (uniform control flow)
-      for (int bin = max(kb, seg_lo); bin < min(kb + nb, seg_hi); bin++) {
-        while (cur < nmel && bin >= seg_s[cur + 1].x) finish_seg();
-        const float2 w = w2_s[bin];
-        const float p = P[(bin - kb) * kDftM + tid];
-        Rcur = fmaf(w.x, p, Rcur);
-        Fcur = fmaf(w.y, p, Fcur);
+      __syncthreads();
+      if (half == 0) {
+        for (int bin = 0; bin < nb; bin++) chk += P[bin * kDftM + row];
+        // ---- fold this tile's bins into the mel bands (uniform control flow)
+        for (int bin = max(kb, seg_lo); bin < min(kb + nb, seg_hi); bin++) {
+          while (cur < nmel && bin >= seg_s[cur + 1].x) finish_seg();
+          const float2 w = w2_s[bin];
+          const float p = P[(bin - kb) * kDftM + row];
+          Rcur = fmaf(w.x, p, Rcur);
+          Fcur = fmaf(w.y, p, Fcur);
+        }
       }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // P reads before later bulk copies
       tc_fence_before();
-      __syncthreads();  // P (aliasing A/B) and the accumulator are free again
+      __syncthreads();  // P (aliasing the stages) and the accumulator are free again
     }
     if (failed) break;
-    while (cur < nmel) finish_seg();
-    if (nmel > 0) emit(nmel - 1, Rprev);
-    if (!isfinite(chk)) {  // a non-finite bin: every band of the frame is NaN -> amin
-      const float val = 10.0f * log10f(a.amin / a.ref);
-      if (valid)
-        for (int m = 0; m < nmel; m++) dst[m] = val;
-      fmax_ = val;
+    if (half == 0) {
+      while (cur < nmel) finish_seg();
+      if (nmel > 0) emit(nmel - 1, Rprev);
+      if (!isfinite(chk)) {  // a non-finite bin: every band of the frame is NaN -> amin
+        const float val = 10.0f * log10f(a.amin / a.ref);
+        if (valid)
+          for (int m = 0; m < nmel; m++) dst[m] = val;
+        fmax_ = val;
+      }
+      if (valid) vmax = fmaxf(vmax, fmax_);
     }
-    if (valid) vmax = fmaxf(vmax, fmax_);
   }
   if (!failed) {
     float m = vmax;

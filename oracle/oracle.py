@@ -10,7 +10,8 @@ It restates MetalMom's CPU algorithm for the path
     centered framing -> periodic Hann -> real FFT -> |X|^2 -> Slaney mel
     -> power_to_db(top_db) -> DCT-II ortho (MFCC)
 
-in float64 NumPy.  Each function cites the Swift source it follows (paths
+and for the features built on it (onset strength, inverse STFT, delta,
+stack_memory) in float64 NumPy.  Each function cites the Swift source it follows (paths
 relative to the MetalMom project root).  The FFT itself is ``numpy.fft.rfft``
 in float64: the reference calls Apple's closed ``vDSP_fft_zrip`` and rescales by
 0.5 so that its output is the plain DFT (``STFT.swift:298-310``); any exact
@@ -318,6 +319,118 @@ def mfcc(y, sr=22050, n_mfcc=20, n_fft=2048, hop=None, win_length=None,
     if D.shape[1] == 0 or k <= 0:
         return np.zeros((max(k, 0), D.shape[1]))
     return dct_basis(k, n_mels) @ D
+
+
+# ---------------------------------------------------------------------------
+# Widening of the path: onset strength, iSTFT, delta, stack_memory
+# ---------------------------------------------------------------------------
+
+def onset_strength(y, sr=22050, n_fft=2048, hop=None, n_mels=128, fmin=0.0,
+                   fmax=None, center=True, aggregate=True, lag=1,
+                   pad_mode=PAD_CONSTANT):
+    """``OnsetDetection.onsetStrength`` (Rhythm/OnsetDetection.swift:23-139).
+
+    Power mel spectrogram (window n_fft, hop default 512) -> power_to_db(ref
+    1, amin 1e-10, top_db 80) -> positive lag difference along time -> mean
+    over bands (or per band), shifted right by ``lag + n_fft // (2 hop)``
+    when centered (``lag`` otherwise) with zeros in front; ``n_frames``
+    columns (``[1, 1]`` / ``[n_mels, 1]`` zeros when there are <= lag frames).
+    """
+    hop = 512 if hop is None else hop
+    S = mel_db(y, sr, n_fft, hop, n_fft, center, n_mels, fmin, fmax, 80.0, pad_mode)
+    n_bands, T = S.shape
+    if T <= lag:
+        return np.zeros((1, 1)) if aggregate else np.zeros((n_bands, 1))
+    diff = np.maximum(0.0, S[:, lag:] - S[:, :-lag])
+    pad = lag + (n_fft // (2 * hop) if center else 0)
+    out_frames = min(diff.shape[1] + pad, T) if center else diff.shape[1] + pad
+    full = np.zeros((n_bands, out_frames))
+    n = min(diff.shape[1], out_frames - pad)
+    if n > 0:
+        full[:, pad:pad + n] = diff[:, :n]
+    return full.mean(axis=0, keepdims=True) if aggregate else full
+
+
+def istft(S, hop=None, win_length=None, center=True, length=None):
+    """``STFT.inverse`` (Spectral/STFT.swift:686-860): inverse real DFT of
+    every frame, synthesis window, overlap-add, division by the overlapped
+    squared windows where their sum exceeds 1e-10, then trimming of the
+    centre padding / ``length``.  ``S`` is complex [n_freqs, n_frames]; a
+    non-power-of-two n_fft gives zeros of the padded length (:719-724)."""
+    S = np.asarray(S)
+    n_freqs, T = S.shape
+    n_fft = (n_freqs - 1) * 2
+    hop = n_fft // 4 if hop is None else hop
+    win = n_fft if win_length is None else win_length
+    expected = n_fft + (T - 1) * hop
+    w = prepare_window(win, n_fft)
+    if not is_power_of_two(n_fft):
+        out = np.zeros(expected)
+    else:
+        X = S.astype(np.complex128).copy()
+        X[0] = X[0].real          # DC and Nyquist: real parts only (:747-753)
+        X[-1] = X[-1].real
+        frames = np.fft.irfft(X.T, n=n_fft, axis=1) * w[None, :]
+        out = np.zeros(expected)
+        wsum = np.zeros(expected)
+        for f in range(T):
+            out[f * hop:f * hop + n_fft] += frames[f]
+            wsum[f * hop:f * hop + n_fft] += w * w
+        nz = wsum > 1e-10
+        out[nz] /= wsum[nz]
+    if center:
+        a = n_fft // 2
+        if length is not None:
+            r = out[a:min(a + length, expected)]
+            return np.concatenate([r, np.zeros(length - len(r))]) if len(r) < length else r
+        b = expected - n_fft // 2
+        return out[a:b] if b > a else np.zeros(0)
+    if length is not None:
+        return out[:length] if len(out) >= length else np.concatenate([out, np.zeros(length - len(out))])
+    return out
+
+
+def savgol_coeffs(width: int, order: int) -> np.ndarray:
+    """Savitzky-Golay derivative coefficients (Features/Delta.swift:30-135):
+    row ``order`` of pinv(V), V[i, j] = (i - width//2)^j, j <= order, times
+    ``order!``; coefficient k multiplies the sample at offset k - width//2."""
+    half = width // 2
+    x = np.arange(width, dtype=np.float64) - half
+    V = np.vander(x, order + 1, increasing=True)
+    return np.linalg.pinv(V)[order] * math.factorial(order)
+
+
+def delta(data, width=9, order=1):
+    """``Delta.compute`` (Features/Delta.swift:137-241), librosa's
+    ``mode='interp'``: interior frames by the SG filter; the first and last
+    ``width//2`` frames take the filter applied to the first / last ``width``
+    frames."""
+    D = np.asarray(data, dtype=np.float64)
+    nf, T = D.shape
+    half = width // 2
+    c = savgol_coeffs(width, order)
+    out = np.zeros_like(D)
+    for t in range(half, T - half):
+        out[:, t] = D[:, t - half:t + half + 1] @ c
+    left = D[:, :width] @ c
+    right = D[:, T - width:] @ c
+    out[:, :half] = left[:, None]
+    out[:, T - half:] = right[:, None]
+    return out
+
+
+def stack_memory(data, n_steps=2, delay=1):
+    """``Delta.stackMemory`` (Features/Delta.swift:256-290): rows
+    ``step*n_features + f`` hold the features delayed by ``step*delay``
+    frames, zeros before the start."""
+    D = np.asarray(data, dtype=np.float64)
+    nf, T = D.shape
+    out = np.zeros((nf * n_steps, T))
+    for step in range(n_steps):
+        sh = step * delay
+        if sh < T:
+            out[step * nf:(step + 1) * nf, sh:] = D[:, :T - sh]
+    return out
 
 
 # ---------------------------------------------------------------------------

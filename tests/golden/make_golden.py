@@ -1,6 +1,7 @@
 """Collect the reference's golden vectors for the spectral front end.
 
-MetalMom pins its STFT / mel / MFCC / dB path against librosa-generated
+MetalMom pins its STFT / mel / MFCC / dB path (and the onset strength and
+delta / stack_memory features built on it) against librosa-generated
 ``.npy`` files (``Tests/golden/``, written by ``scripts/generate_golden.py``
 in the MetalMom project; librosa >= 0.11).  This script copies the files that
 belong to that path into one compressed archive,
@@ -30,6 +31,12 @@ DENSE = [
     "mfcc_440hz_default",
     "mfcc_440hz_13_1024",
     "mfcc_440hz_20_64_fmin300_fmax8000",
+    # widening of the path: onset strength, delta / stack_memory on MFCC
+    "onset_strength_440hz_default",
+    "mfcc",
+    "delta",
+    "delta_delta",
+    "stack_memory",
 ]
 SPARSE = [
     "mel_filterbank_128_2048",

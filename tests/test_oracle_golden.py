@@ -148,3 +148,37 @@ def test_top_db_floor():
     S = rng.random(1000) ** 8
     d = O.power_to_db(S, top_db=30.0)
     assert d.min() >= d.max() - 30.0 - 1e-9
+
+
+# ---------------------------------------------------------------------------
+# widening of the path: onset strength, delta, stack_memory, iSTFT
+# ---------------------------------------------------------------------------
+
+def test_onset_strength_golden():
+    """test_onset_strength.py: librosa.onset.onset_strength(y, sr) defaults."""
+    exp = golden("onset_strength_440hz_default")
+    got = O.onset_strength(signal_440(), SR)
+    assert got.shape == (1, exp.shape[0])
+    np.testing.assert_allclose(got[0], exp, rtol=1e-4, atol=1e-4)
+
+
+def test_delta_and_stack_memory_goldens():
+    """test_parity_delta.py (delta atol/rtol 0.1, delta-delta 0.2, stack 1e-4);
+    held here to 1e-4 absolute."""
+    m = golden("mfcc")
+    np.testing.assert_allclose(O.delta(m), golden("delta"), atol=1e-4, rtol=1e-4)
+    np.testing.assert_allclose(O.delta(m, order=2), golden("delta_delta"), atol=1e-4, rtol=1e-4)
+    np.testing.assert_allclose(O.stack_memory(m, n_steps=3), golden("stack_memory"), atol=1e-6)
+
+
+def test_istft_inverts_the_oracle_stft():
+    """test_parity_istft.py's round trips, as properties: the inverse of the
+    forward transform reconstructs the signal (COLA window-sum division)."""
+    rng = np.random.default_rng(42)
+    for n_fft, L in ((2048, 22050), (1024, 8192), (512, 3001)):
+        y = rng.standard_normal(L)
+        S = O.stft_complex(y, n_fft, n_fft // 4, n_fft, True)
+        r = O.istft(S, n_fft // 4, center=True, length=L)
+        np.testing.assert_allclose(r, y, atol=1e-9)
+        r2 = O.istft(S, n_fft // 4, center=True)
+        assert len(r2) == (S.shape[1] - 1) * (n_fft // 4)

@@ -102,6 +102,28 @@ MM_API int32_t mm_mfcc(mm_context ctx, const float* signal_data, int64_t signal_
  * NULL-safe. */
 MM_API void mm_buffer_free(MMBuffer* buf);
 
+/* ---- Features built on the front end (reference entry points) ---------- */
+
+/* Replaces Bridge.swift:1319 (mm_onset_strength): spectral flux of the
+ * power_to_db(top_db 80) mel spectrogram (lag 1), mean over bands (aggregate
+ * != 0, shape [1, n_frames]) or per band ([n_mels, n_frames]), shifted by
+ * lag + n_fft/(2 hop) when centred.  hop <= 0 -> 512, f_max <= 0 -> sr/2. */
+MM_API int32_t mm_onset_strength(mm_context ctx, const float* signal_data, int64_t signal_length,
+                                 int32_t sample_rate, int32_t n_fft, int32_t hop_length,
+                                 int32_t n_mels, float f_min, float f_max,
+                                 int32_t center, int32_t aggregate, MMBuffer* out);
+
+/* Replaces Bridge.swift:934 (mm_delta): Savitzky-Golay derivative of order
+ * `order` along time of [n_features, n_frames] (librosa mode 'interp'). */
+MM_API int32_t mm_delta(mm_context ctx, const float* data, int64_t count,
+                        int32_t n_features, int32_t n_frames,
+                        int32_t width, int32_t order, MMBuffer* out);
+
+/* Replaces Bridge.swift:959 (mm_stack_memory): [n_features*n_steps, n_frames]. */
+MM_API int32_t mm_stack_memory(mm_context ctx, const float* data, int64_t count,
+                               int32_t n_features, int32_t n_frames,
+                               int32_t n_steps, int32_t delay, MMBuffer* out);
+
 /* ---- Additive entry points (no counterpart in the reference) ----------- */
 
 #define MM_PAD_CONSTANT 0 /* zeros: the reference's centering */

@@ -3,6 +3,7 @@
 // The reference entry points keep MetalMom's validation order, sentinels,
 // status codes, output shapes and ownership rules (Bridge.swift:16-492,
 // 3695-3711); the work itself runs on the CUDA device.
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -258,6 +259,156 @@ int32_t mm_mfcc(mm_context ctx, const float *signal_data, int64_t signal_length,
   }
   fill_buffer(out, data, g.n_mfcc_eff, T);
   return MM_OK;
+}
+
+}  // extern "C"
+
+// Savitzky-Golay derivative coefficients in float64 (Delta.swift:30-135):
+// row `order` of (V^T V)^-1 V^T with V[i][j] = (i - width/2)^j, j <= order,
+// times order!.  False when V^T V is singular.
+static bool savgol_coeffs(int width, int order, float *out) {
+  const int cols = order + 1, half = width / 2;
+  std::vector<double> V((size_t)width * cols), A((size_t)cols * 2 * cols, 0.0);
+  for (int i = 0; i < width; i++) {
+    double p = 1.0;
+    for (int j = 0; j < cols; j++, p *= (double)(i - half)) V[(size_t)i * cols + j] = p;
+  }
+  for (int i = 0; i < cols; i++) {
+    for (int j = 0; j < cols; j++) {
+      double s = 0.0;
+      for (int k = 0; k < width; k++) s += V[(size_t)k * cols + i] * V[(size_t)k * cols + j];
+      A[(size_t)i * 2 * cols + j] = s;
+    }
+    A[(size_t)i * 2 * cols + cols + i] = 1.0;
+  }
+  for (int i = 0; i < cols; i++) {  // Gauss-Jordan with partial pivoting
+    int piv = i;
+    for (int k = i + 1; k < cols; k++)
+      if (fabs(A[(size_t)k * 2 * cols + i]) > fabs(A[(size_t)piv * 2 * cols + i])) piv = k;
+    if (piv != i)
+      for (int j = 0; j < 2 * cols; j++) std::swap(A[(size_t)i * 2 * cols + j], A[(size_t)piv * 2 * cols + j]);
+    const double d = A[(size_t)i * 2 * cols + i];
+    if (fabs(d) <= 1e-15) return false;
+    for (int j = 0; j < 2 * cols; j++) A[(size_t)i * 2 * cols + j] /= d;
+    for (int k = 0; k < cols; k++) {
+      if (k == i) continue;
+      const double f = A[(size_t)k * 2 * cols + i];
+      for (int j = 0; j < 2 * cols; j++) A[(size_t)k * 2 * cols + j] -= f * A[(size_t)i * 2 * cols + j];
+    }
+  }
+  double fact = 1.0;
+  for (int i = 2; i <= order; i++) fact *= (double)i;
+  for (int k = 0; k < width; k++) {
+    double s = 0.0;
+    for (int j = 0; j < cols; j++) s += A[(size_t)order * 2 * cols + cols + j] * V[(size_t)k * cols + j];
+    out[k] = (float)(s * fact);
+  }
+  return true;
+}
+
+// Host matrix in -> kernel -> host matrix out through the thread's workspace.
+template <typename Launch>
+static int32_t run_matrix(const float *data, size_t in_count, size_t out_count, long long rows, long long cols,
+                          MMBuffer *out, Launch launch) {
+  int st = gpu_available();
+  if (st != MM_OK) return st;
+  const size_t in_b = sizeof(float) * in_count, out_b = sizeof(float) * out_count;
+  const size_t in_pad = (in_b + 255) & ~size_t(255);
+  Workspace *ws = nullptr;
+  if ((st = thread_workspace(in_pad + out_b, std::max(in_b, out_b), &ws)) != MM_OK) return st;
+  cudaStream_t s = ws->stream;
+  cudaError_t e = cudaStreamSynchronize(s);
+  float *d_in = reinterpret_cast<float *>(ws->dev), *d_out = reinterpret_cast<float *>(ws->dev + in_pad);
+  if (e == cudaSuccess) {
+    memcpy(ws->host, data, in_b);
+    e = cudaMemcpyAsync(d_in, ws->host, in_b, cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess) e = launch(d_in, d_out, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ws->host, d_out, out_b, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e);
+  float *res = (float *)malloc(out_b);
+  if (!res) return MM_ERR_ALLOC_FAILED;
+  memcpy(res, ws->host, out_b);
+  fill_buffer(out, res, rows, cols);
+  return MM_OK;
+}
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// features on the front end: onset strength, delta, stack_memory
+// ---------------------------------------------------------------------------
+
+// Replaces Bridge.swift:1319-1358 (mm_onset_strength).  Sentinels as there:
+// hop <= 0 -> 512, f_max <= 0 -> sr/2; window n_fft, lag 1, power_to_db with
+// ref 1, amin 1e-10, top_db 80.  Shape [1, n_frames] (aggregate) or
+// [n_mels, n_frames]; [1, 1] / [n_mels, 1] zeros when there are no frames.
+int32_t mm_onset_strength(mm_context ctx, const float *signal_data, int64_t signal_length, int32_t sample_rate,
+                          int32_t n_fft, int32_t hop_length, int32_t n_mels, float f_min, float f_max,
+                          int32_t center, int32_t aggregate, MMBuffer *out) {
+  (void)ctx;  // the reference ignores the context here too
+  if (!signal_data || signal_length <= 0 || !out) return MM_ERR_INVALID_INPUT;
+  if (n_mels <= 0) return MM_ERR_INVALID_INPUT;  // the reference would average over no bands
+  Group g;
+  int st = resolve_mel_group(g, sample_rate, n_fft, hop_length > 0 ? hop_length : 512, n_fft, center, n_mels,
+                             f_min, f_max);
+  if (st != MM_OK) return st;
+  g.mode = MODE_MELDB;
+  g.power = 2.0f;
+  g.amin = 1e-10f;
+  g.ref = 1.0f;
+  g.top_db = 80.0f;
+  g.post = aggregate ? POST_ONSET_MEAN : POST_ONSET_BANDS;
+  g.lag = 1;
+  g.n_mfcc_eff = 0;
+  const int rows = aggregate ? 1 : n_mels;
+  const long long T = frame_count(signal_length, g.n_fft, g.hop, g.center);
+  float *data = nullptr;
+  if (T > 0) {
+    if (!supported_size(g)) return MM_ERR_INVALID_INPUT;
+    st = run_batch(g, &signal_data, &signal_length, 1, &data);
+    if (st != MM_OK) return st;
+    fill_buffer(out, data, rows, T);
+    return MM_OK;
+  }
+  data = (float *)calloc((size_t)rows, sizeof(float));
+  if (!data) return MM_ERR_ALLOC_FAILED;
+  fill_buffer(out, data, rows, 1);
+  return MM_OK;
+}
+
+// Replaces Bridge.swift:934-955 (mm_delta): [n_features, n_frames] in and out.
+// Rejected with MM_ERR_INVALID_INPUT where the reference traps: count !=
+// n_features * n_frames, width even, < 3 or > 63, order < 1 or >= width,
+// n_frames < width.
+int32_t mm_delta(mm_context ctx, const float *data, int64_t count, int32_t n_features, int32_t n_frames,
+                 int32_t width, int32_t order, MMBuffer *out) {
+  (void)ctx;
+  if (!data || count <= 0 || !out || n_features <= 0 || n_frames <= 0) return MM_ERR_INVALID_INPUT;
+  if ((long long)n_features * n_frames != count) return MM_ERR_INVALID_INPUT;
+  if (width < 3 || width % 2 == 0 || width > kDeltaMaxWidth || order < 1 || order >= width || n_frames < width)
+    return MM_ERR_INVALID_INPUT;
+  DeltaCoeffs c{};
+  if (!savgol_coeffs(width, order, c.c)) return MM_ERR_INVALID_INPUT;
+  return run_matrix(data, (size_t)count, (size_t)count, n_features, n_frames, out,
+                    [&](const float *x, float *y, cudaStream_t s) {
+                      return launch_delta(x, y, n_features, n_frames, width, c, s);
+                    });
+}
+
+// Replaces Bridge.swift:959-980 (mm_stack_memory): [n_features * n_steps,
+// n_frames], zeros before the start.
+int32_t mm_stack_memory(mm_context ctx, const float *data, int64_t count, int32_t n_features, int32_t n_frames,
+                        int32_t n_steps, int32_t delay, MMBuffer *out) {
+  (void)ctx;
+  if (!data || count <= 0 || !out || n_features <= 0 || n_frames <= 0 || n_steps <= 0) return MM_ERR_INVALID_INPUT;
+  if ((long long)n_features * n_frames != count) return MM_ERR_INVALID_INPUT;
+  const size_t out_count = (size_t)count * (size_t)n_steps;
+  return run_matrix(data, (size_t)count, out_count, (long long)n_features * n_steps, n_frames, out,
+                    [&](const float *x, float *y, cudaStream_t s) {
+                      return launch_stack_memory(x, y, n_features, n_frames, n_steps, delay, s);
+                    });
 }
 
 // ---------------------------------------------------------------------------

@@ -96,7 +96,36 @@ struct DctArgs {
   float *out;    // per clip [n_mfcc][n_frames] at clips[c].out_off
 };
 
-constexpr int kDctTile = 64;  // frames per DCT tile
+constexpr int kDctTile = 64;  // frames per DCT tile (also the onset kernel's tile)
+
+// What follows the log-mel rows on the MFCC path.
+enum PostStage : int { POST_DCT = 0, POST_ONSET_MEAN = 1, POST_ONSET_BANDS = 2 };
+
+// Onset strength from the frame-major log-mel: out[o] (or out[b][o]) for
+// o = i + shift is the mean over bands (or per band) of
+// max(0, S[i+lag][b] - S[i][b]), S floored at max - top_db; 0 elsewhere.
+struct OnsetArgs {
+  const float *mel_db;
+  const ClipDesc *clips;
+  const int *tile_clip, *tile_first;
+  int total_tiles;
+  const unsigned *clip_max;
+  int n_mels, lag, shift, bands;
+  float top_db;
+  float *out;
+};
+cudaError_t launch_onset(const OnsetArgs &a, cudaStream_t s);
+
+// Savitzky-Golay delta along time of a [n_features x n_frames] matrix
+// (interp edges) and stacked delayed copies (zeros before the start).
+constexpr int kDeltaMaxWidth = 63;
+struct DeltaCoeffs {
+  float c[kDeltaMaxWidth];
+};
+cudaError_t launch_delta(const float *x, float *y, int n_features, int n_frames, int width, DeltaCoeffs c,
+                         cudaStream_t s);
+cudaError_t launch_stack_memory(const float *x, float *y, int n_features, int n_frames, int n_steps, int delay,
+                                cudaStream_t s);
 
 // Frames per CTA tile for a given log2(n_fft) and launch variant.
 int frames_per_tile(int log2n, int variant);

@@ -63,16 +63,16 @@ long long frame_count(long long length, int n_fft, int hop, int center) {
 
 bool same_group(const Group &a, const Group &b) {
   return std::tie(a.mode, a.sr, a.n_fft, a.hop, a.win, a.window_zero, a.center, a.pad_mode, a.n_mels,
-                  a.n_mfcc_eff, a.fmin, a.fmax, a.top_db, a.power, a.amin, a.ref, a.dft_form) ==
+                  a.n_mfcc_eff, a.fmin, a.fmax, a.top_db, a.power, a.amin, a.ref, a.dft_form, a.post, a.lag) ==
          std::tie(b.mode, b.sr, b.n_fft, b.hop, b.win, b.window_zero, b.center, b.pad_mode, b.n_mels,
-                  b.n_mfcc_eff, b.fmin, b.fmax, b.top_db, b.power, b.amin, b.ref, b.dft_form);
+                  b.n_mfcc_eff, b.fmin, b.fmax, b.top_db, b.power, b.amin, b.ref, b.dft_form, b.post, b.lag);
 }
 
 int output_rows(const Group &g) {
   switch (g.mode) {
     case MODE_SPECTRUM: return g.n_fft / 2 + 1;
     case MODE_MEL: return g.n_mels;
-    default: return g.n_mfcc_eff;
+    default: return g.post == POST_ONSET_MEAN ? 1 : (g.post == POST_ONSET_BANDS ? g.n_mels : g.n_mfcc_eff);
   }
 }
 
@@ -289,7 +289,23 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   if (e != cudaSuccess) return e;
   if (grid > 0) launches++;
   if (ev && (e = cudaEventRecord(ev[2], s)) != cudaSuccess) return e;
-  if (g.mode == MODE_MELDB && g.n_mfcc_eff > 0 && !L.dct_tile_clip.empty()) {
+  if (g.mode == MODE_MELDB && g.post != POST_DCT && !L.dct_tile_clip.empty()) {
+    OnsetArgs o;
+    o.mel_db = b.meldb;
+    o.clips = b.clips;
+    o.tile_clip = b.dct_tile_clip;
+    o.tile_first = b.dct_tile_first;
+    o.total_tiles = (int)L.dct_tile_clip.size();
+    o.clip_max = b.clip_max;
+    o.n_mels = g.n_mels;
+    o.lag = g.lag;
+    o.shift = g.lag + (g.center ? g.n_fft / (2 * g.hop) : 0);
+    o.bands = g.post == POST_ONSET_BANDS;
+    o.top_db = g.top_db;
+    o.out = b.out;
+    if ((e = launch_onset(o, s)) != cudaSuccess) return e;
+    launches++;
+  } else if (g.mode == MODE_MELDB && g.n_mfcc_eff > 0 && !L.dct_tile_clip.empty()) {
     DctArgs d;
     d.mel_db = b.meldb;
     d.clips = b.clips;

@@ -26,6 +26,8 @@ struct Group {
   float power = 2.0f, amin = 1e-10f, ref = 1.0f;
   int variant = 0;  // frame-kernel launch variant (autotuned per n_fft)
   int dft_form = DFT_FFT_F32;
+  int post = POST_DCT;  // MODE_MELDB: DCT (MFCC) or onset strength
+  int lag = 1;          // onset difference lag
 };
 
 // Process-wide autotuning table: launch variant per log2(n_fft).

@@ -77,3 +77,28 @@ def power_to_db(S, ref=1.0, amin=1e-10, top_db=80.0):
 def amplitude_to_db(S, ref=1.0, amin=1e-5, top_db=80.0):
     """``20 log10(max(S, amin) / ref)`` floored at ``max - top_db``."""
     return _db("mm_amplitude_to_db", lib.mm_amplitude_to_db, S, ref, amin, top_db)
+
+
+def delta(data, width=9, order=1, axis=-1, **kwargs):
+    """Savitzky-Golay delta of order ``order`` along time of (n_features, n_frames)
+    (mirrors feature.py:1312-1357 of the reference)."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    if data.ndim == 1:
+        data = data.reshape(1, -1)
+    n_features, n_frames = data.shape
+    flat = data.ravel()
+    ptr = ffi.cast("const float*", flat.ctypes.data)
+    return _call("mm_delta", lib.mm_delta, ptr, len(flat), n_features, n_frames, width, order)
+
+
+def stack_memory(data, n_steps=2, delay=1, **kwargs):
+    """Stacked delayed copies (n_features * n_steps, n_frames), zeros before the
+    start (mirrors feature.py:1360-1404 of the reference)."""
+    data = np.ascontiguousarray(data, dtype=np.float32)
+    if data.ndim == 1:
+        data = data.reshape(1, -1)
+    n_features, n_frames = data.shape
+    flat = data.ravel()
+    ptr = ffi.cast("const float*", flat.ctypes.data)
+    return _call("mm_stack_memory", lib.mm_stack_memory, ptr, len(flat), n_features, n_frames,
+                 n_steps, delay)

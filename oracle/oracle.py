@@ -427,9 +427,12 @@ def stack_memory(data, n_steps=2, delay=1):
     nf, T = D.shape
     out = np.zeros((nf * n_steps, T))
     for step in range(n_steps):
-        sh = step * delay
-        if sh < T:
-            out[step * nf:(step + 1) * nf, sh:] = D[:, :T - sh]
+        sh = step * delay  # output frame t takes input frame t - sh
+        rows = slice(step * nf, (step + 1) * nf)
+        if 0 <= sh < T:
+            out[rows, sh:] = D[:, :T - sh]
+        elif -T < sh < 0:
+            out[rows, :T + sh] = D[:, -sh:]
     return out
 
 

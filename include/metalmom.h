@@ -72,6 +72,18 @@ MM_API void mm_destroy(mm_context ctx);
 MM_API int32_t mm_stft(mm_context ctx, const float* signal_data, int64_t signal_length,
                 int32_t sample_rate, const MMSTFTParams* params, MMBuffer* out);
 
+/* Replaces Bridge.swift:144 (mm_istft): inverse STFT by overlap-add of the
+ * windowed inverse transforms, divided by the overlapped squared windows.
+ * stft_data: interleaved complex [n_freqs, n_frames] row-major (stft_count =
+ * 2 * n_freqs * n_frames floats); n_fft = 2 * (n_freqs - 1); centre padding
+ * trimmed when center != 0; output_length > 0 truncates or zero-pads.
+ * Output ndim 1.  hop_length <= 0, n_freqs < 2 or a short stft_count are
+ * rejected (MM_ERR_INVALID_INPUT). */
+MM_API int32_t mm_istft(mm_context ctx, const float* stft_data, int64_t stft_count,
+                        int32_t n_freqs, int32_t n_frames, int32_t sample_rate,
+                        int32_t hop_length, int32_t win_length, int32_t center,
+                        int64_t output_length, MMBuffer* out);
+
 /* Replaces Bridge.swift:225 (mm_amplitude_to_db): 20*log10(max(x,amin)/ref),
  * floored at max-top_db when top_db > 0.  Output ndim 1, shape [count]. */
 MM_API int32_t mm_amplitude_to_db(mm_context ctx, const float* data, int64_t count,

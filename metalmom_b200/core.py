@@ -1,4 +1,4 @@
-"""``stft`` (mirrors MetalMom python/metalmom/core.py:198-250)."""
+"""``stft`` and ``istft`` (mirror MetalMom python/metalmom/core.py:198-319)."""
 
 import numpy as np
 
@@ -29,6 +29,34 @@ def stft(y, n_fft=2048, hop_length=None, win_length=None, center=True):
         status = lib.mm_stft(ctx, ptr, len(y), 22050, params, out)
         if status != 0:
             raise RuntimeError(f"mm_stft failed with status {status}")
+        return buffer_to_numpy(out)
+    finally:
+        lib.mm_destroy(ctx)
+
+
+def istft(stft_matrix, hop_length=None, win_length=None, center=True, length=None):
+    """Inverse STFT of a complex spectrogram (n_fft // 2 + 1, n_frames), computed on
+    the GPU (mirrors MetalMom python/metalmom/core.py:253-319: hop ``n_fft // 4``,
+    window ``n_fft``, 1-D float32 result)."""
+    if not np.iscomplexobj(stft_matrix):
+        stft_matrix = np.asarray(stft_matrix).astype(np.complex64)
+    else:
+        stft_matrix = np.asarray(stft_matrix, dtype=np.complex64)
+    n_freqs, n_frames = stft_matrix.shape
+    n_fft = (n_freqs - 1) * 2
+    hop = hop_length if hop_length is not None else n_fft // 4
+    win = win_length if win_length is not None else n_fft
+    inter = np.ascontiguousarray(stft_matrix).view(np.float32)
+    ctx = lib.mm_init()
+    if ctx == ffi.NULL:
+        raise RuntimeError("Failed to initialize MetalMom context")
+    try:
+        out = ffi.new("MMBuffer*")
+        ptr = ffi.cast("const float*", inter.ctypes.data)
+        status = lib.mm_istft(ctx, ptr, inter.size, n_freqs, n_frames, 22050, hop, win,
+                              1 if center else 0, length if length is not None else 0, out)
+        if status != 0:
+            raise RuntimeError(f"mm_istft failed with status {status}")
         return buffer_to_numpy(out)
     finally:
         lib.mm_destroy(ctx)

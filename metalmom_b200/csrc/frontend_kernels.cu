@@ -1079,6 +1079,86 @@ cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a
   }
 }
 
+// The same product with whole rows: the basis [n_mfcc][n_mels] is staged once
+// per CTA and each 64-frame tile is loaded over all bands at once (one
+// barrier pair per tile).  Row stride n_mels + pad with stride % 32 == 4 keeps
+// the float4 row reads of the 64 frames conflict-free.  n_mels % 4 == 0,
+// n_mels <= 256, n_mfcc <= 32.
+__host__ __device__ inline int dct_row_stride(int n_mels) { return n_mels + ((36 - (n_mels & 31)) & 31); }
+
+template <int KQ>
+__global__ void __launch_bounds__(256, 3) dct_rows_kernel(DctArgs a) {
+  extern __shared__ __align__(16) float dsm[];
+  const int nm = a.n_mels, stride = dct_row_stride(nm), n4 = nm / 4;
+  float *bas = dsm;                      // [4*KQ][nm]
+  float *tile = dsm + 4 * KQ * nm;       // [64][stride]
+  const int tid = threadIdx.x;
+  const int fr = tid & (kDctTile - 1), kg = tid / kDctTile;
+  for (int i = tid; i < 4 * KQ * nm; i += 256) {
+    const int k = i / nm;
+    bas[i] = k < a.n_mfcc ? __ldg(a.basis + i) : 0.0f;
+  }
+  const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * nm);
+  const float4 *trow = reinterpret_cast<const float4 *>(tile + fr * stride);
+  for (int ti = blockIdx.x; ti < a.total_tiles; ti += gridDim.x) {
+    const int c = __ldg(a.tile_clip + ti);
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int tf = __ldg(a.tile_first + ti);
+    const int nt = min(kDctTile, cd.n_frames - tf);
+    const bool floor_on = a.top_db > 0.0f;
+    const float thr = floor_on ? dec_f(__ldg(a.clip_max + c)) - a.top_db : 0.0f;
+    const float4 *src = reinterpret_cast<const float4 *>(a.mel_db + (cd.frame_off + tf) * (long long)nm);
+    __syncthreads();  // the previous tile's reads are done
+    for (int i = tid; i < kDctTile * n4; i += 256) {
+      const int r = i / n4, c4 = i - r * n4;
+      float4 v = r < nt ? __ldg(src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (floor_on && r < nt) {
+        v.x = vthr(v.x, thr);
+        v.y = vthr(v.y, thr);
+        v.z = vthr(v.z, thr);
+        v.w = vthr(v.w, thr);
+      }
+      *reinterpret_cast<float4 *>(tile + r * stride + 4 * c4) = v;
+    }
+    __syncthreads();
+    float acc[KQ];
+#pragma unroll
+    for (int q = 0; q < KQ; q++) acc[q] = 0.0f;
+#pragma unroll 2
+    for (int j = 0; j < n4; j++) {
+      const float4 d = trow[j];
+#pragma unroll
+      for (int q = 0; q < KQ; q++) {
+        const float4 b = brow[q * n4 + j];
+        acc[q] = fmaf(b.x, d.x, acc[q]);
+        acc[q] = fmaf(b.y, d.y, acc[q]);
+        acc[q] = fmaf(b.z, d.z, acc[q]);
+        acc[q] = fmaf(b.w, d.w, acc[q]);
+      }
+    }
+    if (fr < nt) {
+      const long long T = cd.n_frames;
+#pragma unroll
+      for (int q = 0; q < KQ; q++) {
+        const int k = kg * KQ + q;
+        if (k < a.n_mfcc) a.out[cd.out_off + (long long)k * T + tf + fr] = acc[q];
+      }
+    }
+  }
+}
+
+template <int KQ>
+static cudaError_t launch_dct_rows_t(const DctArgs &a, cudaStream_t s) {
+  const size_t smem = sizeof(float) * ((size_t)4 * KQ * a.n_mels + (size_t)kDctTile * dct_row_stride(a.n_mels));
+  int per_sm = 1, sms = 148;
+  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(dct_rows_kernel<KQ>), 256, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = (long long)sms * per_sm;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  dct_rows_kernel<KQ><<<(unsigned)grid, 256, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <int KQ>
 static cudaError_t launch_dct_t(const DctArgs &a, cudaStream_t s) {
   static int sms = 0;
@@ -1093,6 +1173,18 @@ cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
   // 4 coefficient groups x KQ accumulators cover min(n_mfcc, 32) coefficients per pass
   const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
+  if (a.n_mfcc <= kDctKC && a.n_mels % 4 == 0 && a.n_mels <= 256) {
+    switch (kq) {
+      case 1: return launch_dct_rows_t<1>(a, s);
+      case 2: return launch_dct_rows_t<2>(a, s);
+      case 3: return launch_dct_rows_t<3>(a, s);
+      case 4: return launch_dct_rows_t<4>(a, s);
+      case 5: return launch_dct_rows_t<5>(a, s);
+      case 6: return launch_dct_rows_t<6>(a, s);
+      case 7: return launch_dct_rows_t<7>(a, s);
+      default: return launch_dct_rows_t<8>(a, s);
+    }
+  }
   switch (kq) {
     case 1: return launch_dct_t<1>(a, s);
     case 2: return launch_dct_t<2>(a, s);

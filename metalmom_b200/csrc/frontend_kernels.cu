@@ -786,6 +786,68 @@ __global__ void build_mel_seg_kernel(int2 *seg, const int *bin_seg, const int4 *
   ok[1] = good;
 }
 
+// Lane tables of the warp kernel's filterbank walk (one thread).  Lane l of a
+// frame group owns bins [32 l, 32 l + 32) (the last lane also the Nyquist bin
+// M = 32 tpf); it accumulates (R, F) = sum of (w2.x P, w2.y P) and stores the
+// pair in the next "part" slot wherever the segment of bin k differs from that
+// of bin k+1, and after its last bin.  Parts are numbered lane after lane, so
+// the pieces of segment s occupy consecutive slots and segment s+1 starts where
+// s ends.
+//   lw[b * tpf + l]  = w2[32 l + b], b <= 32 (b = 32: Nyquist, last lane only)
+//   lane[l]          = {flush mask over b < 32, first slot of lane l}
+//   band[m]          = first slot of segment m | count(m) << 12 |
+//                      count(m+1) << 18 | NaN flag of band m << 24
+// band m = sum of .x over its own parts + sum of .y over the parts of m+1.
+// ok[2] = 1 when the split holds and the parts fit in `max_slots`.
+__global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const float2 *w2, const int *bin_seg,
+                                      const int2 *seg, int n_mels, int tpf, int max_slots, int *ok) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  ok[2] = 0;
+  if (!ok[1]) return;
+  for (int m = 0; m < n_mels; m++) band[m] = 0;
+  int slot = 0, sid = -1;
+  // segment of bin k: the band of the last bin at or below k that feeds one
+  // (bins with no band carry on the run before them, with zero weights)
+  auto next_sid = [&](int k, int cur) { return bin_seg[k] >= 0 ? bin_seg[k] : cur; };
+  // first(s) accumulates in the low 12 bits of band[s], count(s) in bits 12..17
+  for (int l = 0; l < tpf; l++) {
+    lane[l] = make_int2(0, slot);
+    const int last = (l == tpf - 1) ? 32 : 31;
+    unsigned mask = 0u;
+    for (int b = 0; b <= last; b++) {
+      const int k = 32 * l + b;
+      sid = next_sid(k, sid);
+      lw[b * tpf + l] = w2[k];
+      const bool flush = (b == last) || next_sid(k + 1, sid) != sid;
+      if (!flush) continue;
+      if (b < 32) mask |= 1u << b;
+      if (sid >= 0) {
+        if (slot >= 4096 || sid >= n_mels) return;
+        int w = band[sid];
+        if (((w >> 12) & 63) == 0) w = slot;  // first part of segment sid
+        w += 1 << 12;
+        band[sid] = w;
+      }
+      slot++;
+    }
+    if (l < tpf - 1) lw[32 * tpf + l] = make_float2(0.0f, 0.0f);
+    lane[l].x = (int)mask;
+  }
+  if (slot > max_slots) return;
+  // empty segments start where the next one does; then add count(m+1) and the
+  // NaN flag
+  int next_first = slot;
+  for (int m = n_mels - 1; m >= 0; m--) {
+    if (((band[m] >> 12) & 63) == 0) band[m] = next_first;
+    next_first = band[m] & 4095;
+  }
+  for (int m = 0; m < n_mels; m++) {
+    const int cnt_next = (m + 1 < n_mels) ? ((band[m + 1] >> 12) & 63) : 0;
+    band[m] |= (cnt_next << 18) | ((seg[m].y ? 1 : 0) << 24);
+  }
+  ok[2] = 1;
+}
+
 __global__ void mel_pack_kernel(float *packed, const float *W, const int4 *info, int n_mels, int nfreq) {
   const int m = blockIdx.x;
   if (m >= n_mels) return;
@@ -844,18 +906,27 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
     MM_TRY(cudaMalloc(&t.mel_w, sizeof(float) * (size_t)cnt));
     MM_TRY(cudaMalloc(&t.mel_info, sizeof(int4) * (size_t)n_mels));
     int *bin_seg = nullptr;
-    MM_TRY(cudaMalloc(&d_nnz, 2 * sizeof(int)));
+    MM_TRY(cudaMalloc(&d_nnz, 3 * sizeof(int)));
     MM_TRY(cudaMalloc(&t.mel_w2, sizeof(float2) * (size_t)nfreq));
     MM_TRY(cudaMalloc(&t.mel_seg, sizeof(int2) * (size_t)(n_mels + 1)));
     MM_TRY(cudaMalloc(&bin_seg, sizeof(int) * (size_t)nfreq));
+    const int tpf = mel_lane_tpf(n_fft);
+    if (tpf > 0) {
+      MM_TRY(cudaMalloc(&t.mel_lw, sizeof(float2) * (size_t)(33 * tpf)));
+      MM_TRY(cudaMalloc(&t.mel_lane, sizeof(int2) * (size_t)tpf));
+      MM_TRY(cudaMalloc(&t.mel_band, sizeof(int) * (size_t)n_mels));
+    }
     build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
                                                           (double)fmax);
     build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(t.mel_info, t.mel_w, n_mels, nfreq);
     mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
     build_mel_bins_kernel<<<blocks_for(nfreq, 128), 128, 0, s>>>(t.mel_w2, bin_seg, t.mel_w, n_mels, nfreq);
     build_mel_seg_kernel<<<1, 1, 0, s>>>(t.mel_seg, bin_seg, t.mel_info, n_mels, nfreq, d_nnz);
-    int nnz_ok[2] = {0, 0};
-    e = cudaMemcpyAsync(nnz_ok, d_nnz, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (tpf > 0)
+      build_mel_lane_kernel<<<1, 1, 0, s>>>(t.mel_lw, t.mel_lane, t.mel_band, t.mel_w2, bin_seg, t.mel_seg, n_mels,
+                                            tpf, mel_lane_max_slots(tpf), d_nnz);
+    int nnz_ok[3] = {0, 0, 0};
+    e = cudaMemcpyAsync(nnz_ok, d_nnz, 3 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     cudaFree(d_nnz);
     cudaFree(bin_seg);
@@ -863,6 +934,7 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
     const int nnz = nnz_ok[0];
     t.mel_nnz = nnz;
     t.mel_seg_ok = nnz_ok[1];
+    t.mel_lane_ok = tpf > 0 ? nnz_ok[2] : 0;
     MM_TRY(cudaMalloc(&t.mel_pw, sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)));
     mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
   }
@@ -922,9 +994,13 @@ cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, 
     const long long cnt = (long long)n_mels * nfreq;
     int *d_nnz = nullptr;
     int *bin_seg = nullptr;
-    if (!(t.mel_w = c.take<float>(cnt)) || !(t.mel_info = c.take<int4>(n_mels)) || !(d_nnz = c.take<int>(2)) ||
+    const int tpf = mel_lane_tpf(n_fft);
+    if (!(t.mel_w = c.take<float>(cnt)) || !(t.mel_info = c.take<int4>(n_mels)) || !(d_nnz = c.take<int>(3)) ||
         !(t.mel_w2 = c.take<float2>(nfreq)) || !(t.mel_seg = c.take<int2>(n_mels + 1)) ||
         !(bin_seg = c.take<int>(nfreq)))
+      return cudaErrorMemoryAllocation;
+    if (tpf > 0 && (!(t.mel_lw = c.take<float2>(33 * tpf)) || !(t.mel_lane = c.take<int2>(tpf)) ||
+                    !(t.mel_band = c.take<int>(n_mels))))
       return cudaErrorMemoryAllocation;
     build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(t.mel_w, sr, n_fft, n_mels, (double)fmin,
                                                           (double)fmax);
@@ -932,13 +1008,17 @@ cudaError_t build_tables_at(DevTables &t, char *base, size_t cap, size_t *used, 
     mel_offsets_kernel<<<1, 1, 0, s>>>(t.mel_info, n_mels, d_nnz);
     build_mel_bins_kernel<<<blocks_for(nfreq, 128), 128, 0, s>>>(t.mel_w2, bin_seg, t.mel_w, n_mels, nfreq);
     build_mel_seg_kernel<<<1, 1, 0, s>>>(t.mel_seg, bin_seg, t.mel_info, n_mels, nfreq, d_nnz);
-    int nnz_ok[2] = {0, 0};
-    cudaError_t e = cudaMemcpyAsync(nnz_ok, d_nnz, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (tpf > 0)
+      build_mel_lane_kernel<<<1, 1, 0, s>>>(t.mel_lw, t.mel_lane, t.mel_band, t.mel_w2, bin_seg, t.mel_seg, n_mels,
+                                            tpf, mel_lane_max_slots(tpf), d_nnz);
+    int nnz_ok[3] = {0, 0, 0};
+    cudaError_t e = cudaMemcpyAsync(nnz_ok, d_nnz, 3 * sizeof(int), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return e;
     const int nnz = nnz_ok[0];
     t.mel_nnz = nnz;
     t.mel_seg_ok = nnz_ok[1];
+    t.mel_lane_ok = tpf > 0 ? nnz_ok[2] : 0;
     if (!(t.mel_pw = c.take<float>(nnz))) return cudaErrorMemoryAllocation;
     mel_pack_kernel<<<n_mels, 128, 0, s>>>(t.mel_pw, t.mel_w, t.mel_info, n_mels, nfreq);
   }

@@ -192,6 +192,23 @@ int warp_frames_per_tile(int log2n) {
   }
 }
 
+// Position of bin k in the padded power spectrum (k + min(k / 32, TPF - 1)).
+template <int TPF>
+__device__ __forceinline__ int pad_bin(int k) {
+  const int q = k >> 5;
+  return k + (q < TPF - 1 ? q : TPF - 1);
+}
+
+// mel_dot over the padded power spectrum.
+template <int TPF>
+__device__ __forceinline__ float mel_dot_pad(int4 info, const float *w, const float *P, bool bad) {
+  const float *wr = w + info.z;
+  float acc = 0.0f;
+  for (int q = 0; q < info.y; q++) acc = fmaf(wr[q], P[pad_bin<TPF>(info.x + q)], acc);
+  if (info.w || bad) acc = __int_as_float(0x7fc00000);
+  return acc;
+}
+
 // stage-2 column of slot c for lane l (see the header comment)
 template <int TPF, int C, int c>
 __device__ __forceinline__ int stage2_col(int l) {
@@ -213,8 +230,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nmel = a.n_mels;
-  // Per-bin split of the filterbank (else packed rows).
-  const bool split = a.mel_seg_ok != 0;
+  // Lane walk over the per-bin split of the filterbank (else packed rows).
+  const bool lanes = a.mel_lane_ok != 0;
   const bool mel_in_smem = a.mel_nnz <= kMelSmemMax;
   unsigned char *sp = smem;
   cpx *tw2 = reinterpret_cast<cpx *>(sp);  // W_M^(j k1), [k1-1][j]
@@ -223,11 +240,12 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   sp += align16(size_t(N) * 4);
   cpx *bufs = reinterpret_cast<cpx *>(sp);
   sp += size_t(F) * S::FSTRIDE * 8;
-  int4 *mel_s = reinterpret_cast<int4 *>(sp);  // packed rows: mel_info
-  int2 *seg_s = reinterpret_cast<int2 *>(sp);  // split: mel_seg (n_mels + 1 entries)
-  sp += 16 * (size_t)(nmel + 1);
-  float2 *w2_s = reinterpret_cast<float2 *>(sp);  // split: per-bin weights, M + 1 entries
-  float *melw_s = reinterpret_cast<float *>(sp);  // packed rows
+  // lanes: band words, lane words, lane-minor weights; else packed rows
+  int *band_s = reinterpret_cast<int *>(sp);
+  int2 *lane_s = reinterpret_cast<int2 *>(sp + align16(4 * (size_t)nmel));
+  float2 *lw_s = reinterpret_cast<float2 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);
+  int4 *mel_s = reinterpret_cast<int4 *>(sp);
+  float *melw_s = reinterpret_cast<float *>(sp + 16 * (size_t)nmel);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int grp = lane / TPF;       // frame of this lane within the warp
@@ -240,9 +258,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   }
   for (int i = tid; i < N / 4; i += S::THREADS)
     reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
-  if (split) {
-    for (int i = tid; i <= nmel; i += S::THREADS) seg_s[i] = __ldg(a.mel_seg + i);
-    for (int i = tid; i <= M; i += S::THREADS) w2_s[i] = __ldg(a.mel_w2 + i);
+  if (lanes) {
+    for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
+    for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
+    for (int i = tid; i < 33 * TPF; i += S::THREADS) lw_s[i] = __ldg(a.mel_lw + i);
   } else {
     for (int i = tid; i < nmel; i += S::THREADS) mel_s[i] = __ldg(a.mel_info + i);
     if (mel_in_smem)
@@ -264,7 +283,11 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   }
 
   cpx *fb = bufs + (warp * S::FPW + grp) * S::FSTRIDE;
-  float *P = reinterpret_cast<float *>(fb);
+  // power spectrum, padded: bin k at k + min(k / 32, TPF - 1), so that lane l
+  // of the group reads its bins [32 l, 32 l + 32) at 33 l + b, and the
+  // Nyquist bin M at 33 TPF - 1; group g starts TPF g floats into its buffer
+  // so that the groups of a warp fall in disjoint banks
+  float *P = reinterpret_cast<float *>(fb) + TPF * grp;
   const unsigned gmask = (TPF == 32) ? FULL : (((1u << TPF) - 1u) << (grp * TPF));
 
   const int total = a.total_tiles;
@@ -375,6 +398,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         rcv[m].y = __shfl_sync(FULL, v[16 + m].y, src);
       }
       const bool l0 = (l == 0);
+      float *Pa = P + l;                              // bin l + 32 i at l + 33 i
+      float *Pb = P + (M + TPF - 1 - l) + (l0 ? 1 : 0);  // bin M - l - 32 i, i > 0
       static_for<0, 16>([&](auto ki) {
         constexpr int i = decltype(ki)::value;
         const cpx za = v[i];
@@ -388,14 +413,14 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         const float xr = ex + wr, xi = ey + wi;
         const float yr = ex - wr, yi = ey - wi;
         const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr, yr, yi * yi);
-        const int ka = l + 32 * i;
-        P[ka] = p;
-        P[M - ka] = q;
+        Pa[33 * i] = p;
+        if constexpr (i == 0) Pb[l0 ? -1 : 0] = q;  // lane 0: the Nyquist bin
+        else Pb[-33 * i] = q;
         chk += p + q;
       });
       if (l0) {
         const float p = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
-        P[M / 2] = p;
+        P[M / 2 + TPF / 2] = p;
         chk += p;
       }
     } else {
@@ -428,15 +453,21 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
           const float xr = ex + wr, xi = ey + wi;
           const float yr = ex - wr, yi = ey - wi;
           const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr, yr, yi * yi);
-          P[ka] = p;
-          P[M - ka] = q;
+          if constexpr (cc == 0) {
+            P[l0 ? pad_bin<TPF>(ka) : ka + k2] = p;
+            P[l0 ? pad_bin<TPF>(M - ka) : M - ka + TPF - 1 - k2] = q;
+          } else {
+            // l + TPF cc + 32 k2 with 0 < l + TPF cc < 32: row k2 and row TPF - 1 - k2
+            P[ka + k2] = p;
+            P[M - ka + TPF - 1 - k2] = q;
+          }
           chk += p + q;
         });
       });
       if (l0) {
         const cpx zm = v[TPF / 2];
         const float p = 4.0f * fmaf(zm.x, zm.x, zm.y * zm.y);
-        P[M / 2] = p;
+        P[M / 2 + TPF / 2] = p;
         chk += p;
       }
     }
@@ -445,55 +476,55 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
 
     // ---- log-mel row of this frame + running clip max
     float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
-    if (split) {
-      // band m = R[m] + F[m+1]: lane l sums segment s = it*TPF + l (each bin
-      // read once, two products); F[s+1] comes from the next lane, or for the
-      // group's last lane from lane 0 of the following pass (passes run from
-      // the top band down).
-      const int passes = (nmel + TPF - 1) / TPF;
-      float carry = 0.0f;
-      for (int it = passes - 1; it >= 0; it--) {
-        const int sg = it * TPF + l;
-        float R0 = 0.0f, F0 = 0.0f, R1 = 0.0f, F1 = 0.0f;
-        int nanrow = 0;
-        if (sg < nmel) {
-          const int2 g0 = seg_s[sg];
-          const int k0 = g0.x, k1 = seg_s[sg + 1].x;
-          int k = k0;
-          for (; k + 1 < k1; k += 2) {
-            const float2 wa = w2_s[k], wb = w2_s[k + 1];
-            const float pa = P[k], pb = P[k + 1];
-            R0 = fmaf(wa.x, pa, R0);
-            F0 = fmaf(wa.y, pa, F0);
-            R1 = fmaf(wb.x, pb, R1);
-            F1 = fmaf(wb.y, pb, F1);
-          }
-          if (k < k1) {
-            const float2 wa = w2_s[k];
-            const float pa = P[k];
-            R0 = fmaf(wa.x, pa, R0);
-            F0 = fmaf(wa.y, pa, F0);
-          }
-          nanrow = g0.y;
+    if (lanes) {
+      // lane l sums its 32 bins (the last lane also the Nyquist bin) into
+      // (R, F) = (w.x P, w.y P) and stores the pair in the next part slot at
+      // every segment end; band m then adds the .x of its own parts and the .y
+      // of the parts of segment m + 1 (consecutive slots).
+      float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
+      const int2 li = lane_s[l];
+      const unsigned fl = (unsigned)li.x;
+      int slot = li.y;
+      const float *pl = P + 33 * l;
+      const float2 *wl = lw_s + l;
+      float R = 0.0f, Fs = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 32; b++) {
+        const float p = pl[b];
+        const float2 w = wl[b * TPF];
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        if (fl & (1u << b)) {
+          parts[slot++] = make_float2(R, Fs);
+          R = 0.0f;
+          Fs = 0.0f;
         }
-        const float R = R0 + R1, F = F0 + F1;
-        float Fn = __shfl_down_sync(FULL, F, 1, TPF);
-        const float Ffirst = __shfl_sync(FULL, F, 0, TPF);
-        if (l == TPF - 1) Fn = carry;
-        carry = Ffirst;
-        if (sg < nmel) {
-          float acc = 0.25f * (R + Fn);
-          if (nanrow || bad) acc = __int_as_float(0x7fc00000);
-          const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
-          if (valid) {
-            dst[sg] = val;
-            vmax = fmaxf(vmax, val);
-          }
+      }
+      if (l == TPF - 1) {
+        const float p = pl[32];
+        const float2 w = wl[32 * TPF];
+        parts[slot] = make_float2(fmaf(w.x, p, R), fmaf(w.y, p, Fs));
+      }
+      __syncwarp();
+      for (int m = l; m < nmel; m += TPF) {
+        const int bw = band_s[m];
+        const int first = bw & 4095, cr = (bw >> 12) & 63, cn = cr + ((bw >> 18) & 63);
+        float acc = 0.0f;
+        for (int j = 0; j < cn; j++) {
+          const float2 pv = parts[first + j];
+          acc += j < cr ? pv.x : pv.y;
+        }
+        acc *= 0.25f;
+        if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
+        const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        if (valid) {
+          dst[m] = val;
+          vmax = fmaxf(vmax, val);
         }
       }
     } else {
       for (int m = l; m < nmel; m += TPF) {
-        const float acc = 0.25f * mel_dot(mel_s[m], melw, P, bad);
+        const float acc = 0.25f * mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
         const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
         if (valid) {
           dst[m] = val;
@@ -511,9 +542,9 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
 template <int LOG2N>
 static cudaError_t launch_warp_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using S = WShape<LOG2N>;
-  const size_t split_bytes = align16(8 * (size_t)(S::M + 1));
-  const size_t smem = warp_fixed_smem<LOG2N>() + 16 * (size_t)(a.n_mels + 1) +
-                      std::max(split_bytes, mel_smem_bytes(0, a.mel_nnz));
+  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * 34 * (size_t)S::TPF
+                                      : mel_smem_bytes(a.n_mels, a.mel_nnz);
+  const size_t smem = warp_fixed_smem<LOG2N>() + tables;
   auto kern = frame_warp_kernel<LOG2N>;
   int per_sm = 1, sms = 148;
   cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(kern), S::THREADS, smem, &per_sm, &sms);

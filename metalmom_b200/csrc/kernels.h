@@ -52,6 +52,13 @@ struct DevTables {
   float2 *mel_w2 = nullptr;
   int2 *mel_seg = nullptr;
   int mel_seg_ok = 0;          // 0: the split does not describe the filterbank (use mel_pw)
+  // Lane tables of the same split for the warp kernel (n_fft 256..2048): lane
+  // l of a frame owns bins [32 l, 32 l + 32) and sums them into per-segment
+  // parts (layout at build_mel_lane_kernel).
+  float2 *mel_lw = nullptr;    // [33][n_fft/64] weights, lane-minor
+  int2 *mel_lane = nullptr;    // per lane {flush mask, first part slot}
+  int *mel_band = nullptr;     // per band: first part | counts | NaN flag
+  int mel_lane_ok = 0;
   // DFT-as-GEMM form only: the windowed DFT basis as bf16 hi/lo images and an
   // error word the kernel sets when a bounded wait runs out.
   __nv_bfloat16 *dft_basis = nullptr;
@@ -76,6 +83,10 @@ struct FrontArgs {
   const float2 *mel_w2;  // per-bin split (see DevTables)
   const int2 *mel_seg;
   int mel_seg_ok;
+  const float2 *mel_lw;  // lane tables (see DevTables)
+  const int2 *mel_lane;
+  const int *mel_band;
+  int mel_lane_ok;
   int n_mels;
   float power;  // exponent applied to |X| (2 = power spectrum)
   float amin, ref;
@@ -134,6 +145,13 @@ int frame_variants(int log2n, int mode, int power_is_2);
 // Launch variant 3: the warp-per-frame kernel (MODE_MELDB, n_fft 256..2048).
 constexpr int kWarpVariant = 3;
 int warp_frames_per_tile(int log2n);  // 0 when the size has no warp kernel
+// Lanes per frame of the warp kernel (n_fft / 64) for n_fft 256..2048, else 0.
+inline int mel_lane_tpf(int n_fft) {
+  return (n_fft >= 256 && n_fft <= 2048 && (n_fft & (n_fft - 1)) == 0) ? n_fft / 64 : 0;
+}
+// Filterbank part slots that fit in a frame buffer (66 tpf floats) behind the
+// padded spectrum (33 tpf floats, starting tpf g floats in for frame group g).
+inline int mel_lane_max_slots(int tpf) { return tpf > 0 ? (33 * tpf - tpf * (32 / tpf - 1)) / 2 : 0; }
 cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,
                                  int *launched);
 // Stockham twiddle table length (entries) for log2(n_fft) >= 5.

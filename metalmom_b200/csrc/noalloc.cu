@@ -172,6 +172,10 @@ extern "C" MM_API int32_t mm_mfcc_noalloc(const float *d_signal, int64_t signal_
   a.mel_w2 = t.mel_w2;
   a.mel_seg = t.mel_seg;
   a.mel_seg_ok = t.mel_seg_ok;
+  a.mel_lw = t.mel_lw;
+  a.mel_lane = t.mel_lane;
+  a.mel_band = t.mel_band;
+  a.mel_lane_ok = t.mel_lane_ok;
   a.n_mels = g.n_mels;
   a.power = 2.0f;
   a.amin = g.amin;

@@ -136,6 +136,9 @@ const DevTables *get_tables(const Group &g, int *status) {
     cudaFree(t->mel_info);
     cudaFree(t->mel_w2);
     cudaFree(t->mel_seg);
+    cudaFree(t->mel_lw);
+    cudaFree(t->mel_lane);
+    cudaFree(t->mel_band);
     cudaFree(t->dct);
     cudaFree(t->dft_basis);
     cudaFree(t->dft_err);
@@ -275,6 +278,10 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.mel_w2 = t->mel_w2;
   a.mel_seg = t->mel_seg;
   a.mel_seg_ok = t->mel_seg_ok;
+  a.mel_lw = t->mel_lw;
+  a.mel_lane = t->mel_lane;
+  a.mel_band = t->mel_band;
+  a.mel_lane_ok = t->mel_lane_ok;
   a.n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
   a.power = g.power;
   a.amin = g.amin;

@@ -72,6 +72,17 @@ MM_API void mm_destroy(mm_context ctx);
 MM_API int32_t mm_stft(mm_context ctx, const float* signal_data, int64_t signal_length,
                 int32_t sample_rate, const MMSTFTParams* params, MMBuffer* out);
 
+/* Additive: the C-ABI form of STFT.computeComplex (Spectral/STFT.swift:512-668).
+ * X[k] of each zero-centre-padded windowed frame, the imaginary parts of DC and
+ * Nyquist set to 0.  out: float32 [n_fft/2+1, n_frames, 2] (interleaved re, im;
+ * exactly the stft_data layout mm_istft takes), ndim 3, count 2 * n_freqs *
+ * n_frames.  hop_length <= 0 -> n_fft / 4 and win_length <= 0 -> n_fft (the
+ * defaults of computeComplex).  A non-power-of-two n_fft or a signal shorter
+ * than one frame gives MM_OK with n_frames = 0, as computeComplex returns an
+ * empty [n_freqs, 0] signal. */
+MM_API int32_t mm_stft_complex(mm_context ctx, const float* signal_data, int64_t signal_length,
+                int32_t sample_rate, const MMSTFTParams* params, MMBuffer* out);
+
 /* Replaces Bridge.swift:144 (mm_istft): inverse STFT by overlap-add of the
  * windowed inverse transforms, divided by the overlapped squared windows.
  * stft_data: interleaved complex [n_freqs, n_frames] row-major (stft_count =

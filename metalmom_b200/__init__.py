@@ -7,12 +7,12 @@ batched, device-resident path and ``Server`` a continuously batching request
 loop.
 """
 
-from .core import istft, stft
+from .core import istft, stft, stft_complex
 from .feature import amplitude_to_db, delta, melspectrogram, mfcc, power_to_db, stack_memory
 from .onset import onset_strength
 from .batch import Plan, autotune, frontend_params, mfcc_batch, tune_get, tune_set
 from .serve import Server
 
-__all__ = ["stft", "istft", "melspectrogram", "mfcc", "power_to_db", "amplitude_to_db", "onset_strength",
+__all__ = ["stft", "stft_complex", "istft", "melspectrogram", "mfcc", "power_to_db", "amplitude_to_db", "onset_strength",
            "delta", "stack_memory",
            "mfcc_batch", "Plan", "frontend_params", "autotune", "tune_get", "tune_set", "Server"]

@@ -34,6 +34,37 @@ def stft(y, n_fft=2048, hop_length=None, win_length=None, center=True):
         lib.mm_destroy(ctx)
 
 
+def stft_complex(y, n_fft=2048, hop_length=None, win_length=None, center=True):
+    """Complex STFT, complex64 (n_fft // 2 + 1, n_frames), computed on the GPU.
+
+    The Python form of MetalMom's ``STFT.computeComplex``
+    (Sources/MetalMomCore/Spectral/STFT.swift:512-668): zero centre padding,
+    hop ``n_fft // 4`` and window ``n_fft`` by default, DC and Nyquist real.
+    ``istft(stft_complex(y))`` reconstructs ``y``.
+    """
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    hop = hop_length if hop_length is not None else n_fft // 4
+    win = win_length if win_length is not None else n_fft
+    ctx = lib.mm_init()
+    if ctx == ffi.NULL:
+        raise RuntimeError("Failed to initialize MetalMom context")
+    try:
+        params = ffi.new("MMSTFTParams*")
+        params.n_fft = n_fft
+        params.hop_length = hop
+        params.win_length = win
+        params.center = 1 if center else 0
+        out = ffi.new("MMBuffer*")
+        ptr = ffi.cast("const float*", y.ctypes.data)
+        status = lib.mm_stft_complex(ctx, ptr, len(y), 22050, params, out)
+        if status != 0:
+            raise RuntimeError(f"mm_stft_complex failed with status {status}")
+        inter = buffer_to_numpy(out)  # [n_freqs, n_frames, 2] float32
+        return np.ascontiguousarray(inter).view(np.complex64)[..., 0]
+    finally:
+        lib.mm_destroy(ctx)
+
+
 def istft(stft_matrix, hop_length=None, win_length=None, center=True, length=None):
     """Inverse STFT of a complex spectrogram (n_fft // 2 + 1, n_frames), computed on
     the GPU (mirrors MetalMom python/metalmom/core.py:253-319: hop ``n_fft // 4``,

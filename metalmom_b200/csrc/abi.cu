@@ -169,6 +169,47 @@ int32_t mm_stft(mm_context ctx, const float *signal_data, int64_t signal_length,
   return MM_OK;
 }
 
+// Complex STFT (additive; the C-ABI form of STFT.computeComplex,
+// Spectral/STFT.swift:512-668): zero centre padding, the analysis window of
+// mm_stft, X[k] = sum_n x[n] w[n] e^{-2 pi i k n / n_fft} with the imaginary
+// parts of DC and Nyquist set to 0.  out: float32 [n_freqs][n_frames][2]
+// (interleaved re, im: the layout mm_istft takes), ndim 3.  hop_length <= 0
+// and win_length <= 0 take computeComplex's defaults (n_fft / 4, n_fft).  A
+// non-power-of-two n_fft, or a signal shorter than one frame, gives MM_OK with
+// shape [n_freqs, 0, 2], as computeComplex returns an empty [n_freqs, 0] signal.
+int32_t mm_stft_complex(mm_context ctx, const float *signal_data, int64_t signal_length, int32_t sample_rate,
+                        const MMSTFTParams *params, MMBuffer *out) {
+  if (!ctx || !signal_data || signal_length <= 0 || !params || !out) return MM_ERR_INVALID_INPUT;
+  const int n_fft = params->n_fft;
+  if (n_fft <= 0) return MM_ERR_INVALID_INPUT;
+  const long long nfreq = n_fft / 2 + 1;
+  Group g;
+  g.mode = MODE_COMPLEX;
+  g.power = 1.0f;
+  g.sr = sample_rate;
+  g.n_fft = n_fft;
+  g.log2n = is_pow2(n_fft) ? ilog2(n_fft) : 0;
+  g.hop = params->hop_length > 0 ? params->hop_length : n_fft / 4;
+  g.win = params->win_length > 0 ? params->win_length : n_fft;
+  g.window_zero = 0;
+  g.center = params->center != 0;
+  g.n_mels = 0;
+  g.n_mfcc_eff = 0;
+  if (g.hop <= 0) return MM_ERR_INVALID_INPUT;
+  const long long T = is_pow2(n_fft) ? frame_count(signal_length, n_fft, g.hop, g.center) : 0;
+  if (T > 0 && !supported_size(g)) return MM_ERR_INVALID_INPUT;
+  float *data = nullptr;
+  if (T > 0) {
+    int st = run_batch(g, &signal_data, &signal_length, 1, &data);
+    if (st != MM_OK) return st;
+  }
+  fill_buffer(out, data, nfreq, T);
+  out->ndim = 3;
+  out->shape[2] = 2;
+  out->count = 2 * nfreq * T;
+  return MM_OK;
+}
+
 static int32_t db_common(const float *data, int64_t count, float mult, float ref, float amin,
                          float top_db, MMBuffer *out) {
   if (!data || count <= 0 || !out) return MM_ERR_INVALID_INPUT;

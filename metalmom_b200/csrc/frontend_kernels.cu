@@ -188,8 +188,8 @@ frontend_kernel(FrontArgs a) {
   constexpr int F = Cfg<LOG2N, V>::F;
   constexpr int N = S::N, M = S::M, TPF = S::TPF, THREADS = TPF * F;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int nmel = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
-  const bool mel_in_smem = (MODE != MODE_SPECTRUM) && a.mel_nnz <= kMelSmemMax;
+  const int nmel = mode_has_mel(MODE) ? a.n_mels : 0;
+  const bool mel_in_smem = mode_has_mel(MODE) && a.mel_nnz <= kMelSmemMax;
   unsigned char *sp = smem;
   int4 *mel_s = reinterpret_cast<int4 *>(sp);
   sp += 16 * (size_t)nmel;
@@ -308,6 +308,54 @@ frontend_kernel(FrontArgs a) {
     }
 
     // ---- real split: X[k] = E + W^k O, X[M-k] = conj(E - W^k O)
+    if constexpr (MODE == MODE_COMPLEX) {
+      // the bins themselves, staged in the frame buffer (bin k at slot k) and
+      // written [k][t] by the whole CTA; DC and Nyquist carry no imaginary part
+      cpx xa[8], xb[8];
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int k = j + i * TPF;
+        if (k == 0) {
+          const cpx z = fb[0];
+          xa[i] = {z.x + z.y, 0.0f};
+          xb[i] = {z.x - z.y, 0.0f};
+        } else {
+          const cpx za = fb[padx(k)], zb = fb[padx(M - k)];
+          const cpx E = {0.5f * (za.x + zb.x), 0.5f * (za.y - zb.y)};
+          const cpx O = {0.5f * (za.y + zb.y), -0.5f * (za.x - zb.x)};
+          const cpx WO = cmul(twn[k], O);
+          xa[i] = {E.x + WO.x, E.y + WO.y};
+          xb[i] = {E.x - WO.x, -(E.y - WO.y)};
+        }
+      }
+      cpx xmid = {0.0f, 0.0f};
+      if (j == 0) {
+        const cpx z = fb[padx(M / 2)];
+        xmid = {z.x, -z.y};
+      }
+      frame_sync<TPF>(f);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int k = j + i * TPF;
+        fb[k] = xa[i];
+        fb[M - k] = xb[i];
+      }
+      if (j == 0) fb[M / 2] = xmid;
+      __syncthreads();
+      const long long T = cd.n_frames;
+      const cpx *X0 = buf;
+      float2 *dst = reinterpret_cast<float2 *>(a.out + cd.out_off);
+      for (int it = tid; it < F * (M + 1); it += THREADS) {
+        const int fi = it % F, k = it / F;
+        const int tt = t0 + fi;
+        if (tt < cd.n_frames) {
+          const cpx x = X0[fi * S::FSTRIDE + k];
+          dst[(long long)k * T + tt] = make_float2(x.x, x.y);
+        }
+      }
+      __syncthreads();  // the next tile overwrites buf
+      continue;
+    }
     float pa[8], pb[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
@@ -399,14 +447,15 @@ frontend_kernel(FrontArgs a) {
 template <int MODE, int PW>
 __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_fft) {
   constexpr int F = 128, THREADS = 128, PST = 9;
-  __shared__ float P_s[F * PST];
+  constexpr int CW = (MODE == MODE_COMPLEX) ? 2 : 1;  // floats per bin
+  __shared__ __align__(8) float P_s[F * PST * CW];
   __shared__ int bad_s[F];
   __shared__ float red_s[32];
   extern __shared__ __align__(16) unsigned char smem[];
-  const int nmel = (MODE == MODE_SPECTRUM) ? 0 : a.n_mels;
+  const int nmel = mode_has_mel(MODE) ? a.n_mels : 0;
   int4 *mel_s = reinterpret_cast<int4 *>(smem);
   float *melw_s = reinterpret_cast<float *>(smem + 16 * (size_t)nmel);
-  const bool mel_in_smem = (MODE != MODE_SPECTRUM) && a.mel_nnz <= kMelSmemMax;
+  const bool mel_in_smem = mode_has_mel(MODE) && a.mel_nnz <= kMelSmemMax;
   const int tid = threadIdx.x;
   for (int i = tid; i < nmel; i += THREADS) mel_s[i] = __ldg(a.mel_info + i);
   if (mel_in_smem)
@@ -423,6 +472,35 @@ __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_f
 #pragma unroll
     for (int n = 0; n < 16; n++)
       xw[n] = (n < n_fft) ? sample_at(sig, s0 + n, cd.length, a.pad_mode) * __ldg(a.window + n) : 0.0f;
+    if constexpr (MODE == MODE_COMPLEX) {
+      float2 x[PST];
+#pragma unroll
+      for (int k = 0; k < PST; k++) {
+        float re = 0.0f, im = 0.0f;
+        if (k < nfreq) {
+          for (int n = 0; n < n_fft; n++) {
+            const float2 w = __ldg(a.tw_tiny + ((n * k) % n_fft));
+            re = fmaf(xw[n], w.x, re);
+            im = fmaf(xw[n], w.y, im);
+          }
+        }
+        if (k == 0 || 2 * k == n_fft) im = 0.0f;  // DC and Nyquist are real
+        x[k] = make_float2(re, im);
+      }
+      __syncthreads();
+      float2 *X_s = reinterpret_cast<float2 *>(P_s);
+#pragma unroll
+      for (int k = 0; k < PST; k++) X_s[tid * PST + k] = x[k];
+      __syncthreads();
+      const long long T = cd.n_frames;
+      float2 *dst = reinterpret_cast<float2 *>(a.out + cd.out_off);
+      for (int it = tid; it < F * nfreq; it += THREADS) {
+        const int fi = it % F, k = it / F;
+        const int tt = t0 + fi;
+        if (tt < cd.n_frames) dst[(long long)k * T + tt] = X_s[fi * PST + k];
+      }
+      continue;
+    }
     float p[PST];
     float chk = 0.0f;
 #pragma unroll
@@ -1097,7 +1175,7 @@ template <int LOG2N, int V, int MODE, int PW>
 static cudaError_t launch_fft_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using C = Cfg<LOG2N, V>;
   const size_t smem = fixed_smem_bytes<LOG2N, C::F>() +
-                      (MODE == MODE_SPECTRUM ? 0 : mel_smem_bytes(a.n_mels, a.mel_nnz));
+                      (mode_has_mel(MODE) ? mel_smem_bytes(a.n_mels, a.mel_nnz) : 0);
   static size_t configured = 0;
   return launch_persistent<false>(frontend_kernel<LOG2N, V, MODE, PW>, C::THREADS, smem, a.total_tiles,
                                   grid_limit, &configured, a, s, launched, 1 << LOG2N);
@@ -1130,7 +1208,7 @@ static cudaError_t launch_mode(int log2n, int v, const FrontArgs &a, int grid_li
     default: break;
   }
   if (log2n < 0 || log2n > 4) return cudaErrorInvalidValue;
-  const size_t smem = (MODE == MODE_SPECTRUM) ? 0 : mel_smem_bytes(a.n_mels, a.mel_nnz);
+  const size_t smem = mode_has_mel(MODE) ? mel_smem_bytes(a.n_mels, a.mel_nnz) : 0;
   static size_t configured = 0;
   return launch_persistent<true>(frontend_tiny_kernel<MODE, PW>, 128, smem, a.total_tiles, grid_limit,
                                  &configured, a, s, launched, 1 << log2n);
@@ -1150,6 +1228,7 @@ cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a
       if (pw == 0) return launch_mode<MODE_MEL, 0>(log2n, variant, a, grid_limit, s, launched);
       if (pw == 1) return launch_mode<MODE_MEL, 1>(log2n, variant, a, grid_limit, s, launched);
       return launch_mode<MODE_MEL, 2>(log2n, variant, a, grid_limit, s, launched);
+    case MODE_COMPLEX: return launch_mode<MODE_COMPLEX, 0>(log2n, variant, a, grid_limit, s, launched);
     case MODE_MELDB:
       if (pw != 0) return cudaErrorInvalidValue;
       if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0)

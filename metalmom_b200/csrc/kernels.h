@@ -21,7 +21,11 @@ enum FrontMode : int {
   MODE_SPECTRUM = 0,  // |X|^power per bin -> out[k][t]          (mm_stft)
   MODE_MEL = 1,       // mel of |X|^power  -> out[m][t]           (mm_mel_spectrogram)
   MODE_MELDB = 2,     // 10 log10(max(mel,amin)/ref) -> out[frame][m] + per-clip max
+  MODE_COMPLEX = 3,   // X[k] as (re, im)  -> out[k][t][2]        (mm_stft_complex)
 };
+
+// Modes that project onto the mel filterbank (the others write bins).
+__host__ __device__ constexpr bool mode_has_mel(int mode) { return mode == MODE_MEL || mode == MODE_MELDB; }
 
 enum PadMode : int { PAD_CONSTANT = 0, PAD_REFLECT = 1 };
 

@@ -71,6 +71,7 @@ bool same_group(const Group &a, const Group &b) {
 int output_rows(const Group &g) {
   switch (g.mode) {
     case MODE_SPECTRUM: return g.n_fft / 2 + 1;
+    case MODE_COMPLEX: return 2 * (g.n_fft / 2 + 1);  // interleaved (re, im) per bin
     case MODE_MEL: return g.n_mels;
     default: return g.post == POST_ONSET_MEAN ? 1 : (g.post == POST_ONSET_BANDS ? g.n_mels : g.n_mfcc_eff);
   }
@@ -100,7 +101,7 @@ const DevTables *get_tables(const Group &g, int *status) {
     *status = cuda_status(e);
     return nullptr;
   }
-  const int n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
+  const int n_mels = mode_has_mel(g.mode) ? g.n_mels : 0;
   const int n_mfcc = (g.mode == MODE_MELDB) ? g.n_mfcc_eff : 0;
   TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax, g.dft_form != 0 ? 1 : 0};
   std::lock_guard<std::mutex> lock(g_table_mu);
@@ -282,7 +283,7 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.mel_lane = t->mel_lane;
   a.mel_band = t->mel_band;
   a.mel_lane_ok = t->mel_lane_ok;
-  a.n_mels = (g.mode == MODE_SPECTRUM) ? 0 : g.n_mels;
+  a.n_mels = mode_has_mel(g.mode) ? g.n_mels : 0;
   a.power = g.power;
   a.amin = g.amin;
   a.ref = g.ref;

@@ -149,6 +149,32 @@ MM_API int32_t mm_stack_memory(mm_context ctx, const float* data, int64_t count,
 
 /* ---- Additive entry points (no counterpart in the reference) ----------- */
 
+/* melspectrogram(S=...) on the GPU (python/metalmom/feature.py:50-57 applies
+ * the `_mel_fb.py` filterbank to S with numpy).  S: [n_freqs, n_frames]
+ * row-major, n_freqs == n_fft/2 + 1 (else MM_ERR_INVALID_INPUT, where numpy's
+ * matmul raises); f_max <= 0 -> sr/2.  out: [n_mels, n_frames]; a frame whose
+ * column holds a non-finite value is NaN in every band, as in the dense
+ * product. */
+MM_API int32_t mm_mel_project(mm_context ctx, const float* S, int64_t count, int32_t n_freqs,
+                              int32_t n_frames, int32_t sample_rate, int32_t n_fft, int32_t n_mels,
+                              float f_min, float f_max, MMBuffer* out);
+
+/* mfcc(S=...) on the GPU (feature.py:130-134: scipy dct(S, axis=0, type=2,
+ * norm='ortho')[:n_mfcc]).  S: [n_rows, n_frames]; out: [min(n_out, n_rows),
+ * n_frames].  No top_db floor. */
+MM_API int32_t mm_dct_ortho(mm_context ctx, const float* S, int64_t count, int32_t n_rows,
+                            int32_t n_frames, int32_t n_out, MMBuffer* out);
+
+/* power_to_db / amplitude_to_db of a DEVICE buffer on the caller's stream
+ * (cudaStream_t as void*; asynchronous).  ref_mode 0: divide by `ref`;
+ * ref_mode 1: by max(d_in) computed on the device, as ref=np.max
+ * (feature.py:247-248), NaN when d_in holds a NaN.  top_db <= 0: no floor.
+ * d_out may equal d_in. */
+MM_API int32_t mm_power_to_db_device(const float* d_in, int64_t count, float ref, int32_t ref_mode,
+                                     float amin, float top_db, float* d_out, void* stream);
+MM_API int32_t mm_amplitude_to_db_device(const float* d_in, int64_t count, float ref, int32_t ref_mode,
+                                         float amin, float top_db, float* d_out, void* stream);
+
 #define MM_PAD_CONSTANT 0 /* zeros: the reference's centering */
 #define MM_PAD_REFLECT 1  /* mirror without repeating the edge sample */
 

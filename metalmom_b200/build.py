@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libmetalmom.so")
-SOURCES = ["frontend_kernels.cu", "frontend_warp.cu", "runtime.cu", "abi.cu", "noalloc.cu", "server.cu", "plan.cu", "dft_gemm.cu", "features.cu", "istft.cu"]
+SOURCES = ["frontend_kernels.cu", "frontend_warp.cu", "runtime.cu", "abi.cu", "noalloc.cu", "server.cu", "plan.cu", "dft_gemm.cu", "features.cu", "istft.cu", "spec_ops.cu"]
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-fvisibility=hidden",

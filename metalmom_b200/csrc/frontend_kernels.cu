@@ -669,10 +669,13 @@ __global__ void __launch_bounds__(256) dct_kernel(DctArgs a) {
 // ---------------------------------------------------------------------------
 // dB scaling over a flat array (mm_power_to_db / mm_amplitude_to_db)
 // ---------------------------------------------------------------------------
+// ref_slot (optional): {encoded max of x, NaN flag} written by db_ref_kernel;
+// the reference value is then max(x) (NaN when x holds one), as ref=np.max.
 __global__ void __launch_bounds__(256) db_pass1_kernel(const float *x, float *y, long long n,
                                                        float mult, float amin, float ref,
-                                                       unsigned *slot) {
+                                                       const unsigned *ref_slot, unsigned *slot) {
   __shared__ float red[8];
+  if (ref_slot) ref = ref_slot[1] ? __int_as_float(0x7fc00000) : dec_f(ref_slot[0]);
   float vmax = -INFINITY;
   for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
     const float v = mult * log10f(vthr(x[i], amin) / ref);
@@ -688,6 +691,28 @@ __global__ void __launch_bounds__(256) db_pass1_kernel(const float *x, float *y,
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (threadIdx.x == 0 && v > -INFINITY) atomicMax(slot, enc_f(v));
+  }
+}
+
+__global__ void __launch_bounds__(256) db_ref_kernel(const float *x, long long n, unsigned *ref_slot) {
+  __shared__ float red[8];
+  float vmax = -INFINITY;
+  bool nan = false;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const float v = x[i];
+    nan |= isnan(v);
+    vmax = fmaxf(vmax, v);
+  }
+  if (__syncthreads_or(nan) && threadIdx.x == 0) atomicOr(ref_slot + 1, 1u);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    float v = threadIdx.x < 8 ? red[threadIdx.x] : -INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) atomicMax(ref_slot, enc_f(v));
   }
 }
 
@@ -1022,6 +1047,26 @@ cudaError_t build_tables(DevTables &t, int sr, int n_fft, int win, int n_mels, f
                                                                                       n_mels);
   }
 #undef MM_TRY
+  return cudaGetLastError();
+}
+
+// The dense filterbank [n_mels][n_fft/2+1] and its row info alone (the
+// projection of a given spectrogram); n_fft need not be a power of two.
+cudaError_t build_mel_dense(float *W, int4 *info, int sr, int n_fft, int n_mels, float fmin, float fmax,
+                            cudaStream_t s) {
+  const int nfreq = n_fft / 2 + 1;
+  const long long cnt = (long long)n_mels * nfreq;
+  if (cnt <= 0) return cudaSuccess;
+  build_mel_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(W, sr, n_fft, n_mels, (double)fmin, (double)fmax);
+  build_mel_info_kernel<<<blocks_for(n_mels, 128), 128, 0, s>>>(info, W, n_mels, nfreq);
+  return cudaGetLastError();
+}
+
+// DCT-II ortho basis [n_out][n_rows] (float64-built, as the MFCC tables).
+cudaError_t build_dct_basis_rows(float *B, int n_out, int n_rows, cudaStream_t s) {
+  const long long cnt = (long long)n_out * n_rows;
+  if (cnt <= 0) return cudaSuccess;
+  build_dct_kernel<<<blocks_for(cnt, 256), 256, 0, s>>>(B, n_out, n_rows);
   return cudaGetLastError();
 }
 
@@ -1373,13 +1418,19 @@ cudaError_t launch_fill_pattern(float *p, long long n, cudaStream_t s) {
 }
 
 cudaError_t launch_db(const float *x, float *y, long long n, float mult, float amin, float ref,
-                      float top_db, unsigned *slot, cudaStream_t s) {
+                      float top_db, unsigned *slot, cudaStream_t s, unsigned *ref_slot) {
   if (n <= 0) return cudaSuccess;
   cudaError_t e = launch_fill_u32(slot, encode_max_init(), 1, s);
   if (e != cudaSuccess) return e;
   long long g = (n + 255) / 256;
   if (g > 148 * 16) g = 148 * 16;
-  db_pass1_kernel<<<(unsigned)g, 256, 0, s>>>(x, y, n, mult, amin, ref, slot);
+  if (ref_slot) {
+    if ((e = launch_fill_u32(ref_slot, encode_max_init(), 1, s)) != cudaSuccess) return e;
+    if ((e = launch_fill_u32(ref_slot + 1, 0u, 1, s)) != cudaSuccess) return e;
+    db_ref_kernel<<<(unsigned)g, 256, 0, s>>>(x, n, ref_slot);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  db_pass1_kernel<<<(unsigned)g, 256, 0, s>>>(x, y, n, mult, amin, ref, ref_slot, slot);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (top_db > 0.0f) {
     db_pass2_kernel<<<(unsigned)g, 256, 0, s>>>(y, n, top_db, slot);

@@ -194,8 +194,13 @@ cudaError_t launch_fill_pattern(float *p, long long n, cudaStream_t s);
 
 // dB scaling over a flat array: pass 1 writes mult*log10(max(x,amin)/ref) and the
 // encoded max into *slot; pass 2 floors at max - top_db.
+// ref_slot (2 words, optional): take the reference value as max(x) on the device.
 cudaError_t launch_db(const float *x, float *y, long long n, float mult, float amin,
-                      float ref, float top_db, unsigned *slot, cudaStream_t s);
+                      float ref, float top_db, unsigned *slot, cudaStream_t s,
+                      unsigned *ref_slot = nullptr);
+cudaError_t build_mel_dense(float *W, int4 *info, int sr, int n_fft, int n_mels, float fmin, float fmax,
+                            cudaStream_t s);
+cudaError_t build_dct_basis_rows(float *B, int n_out, int n_rows, cudaStream_t s);
 
 unsigned encode_max_init();  // encoding of -inf
 float decode_max(unsigned u);  // host-side inverse of the max encoding

@@ -321,6 +321,21 @@ def mfcc(y, sr=22050, n_mfcc=20, n_fft=2048, hop=None, win_length=None,
     return dct_basis(k, n_mels) @ D
 
 
+def mel_project(S, sr=22050, n_fft=2048, n_mels=128, fmin=0.0, fmax=None):
+    """``melspectrogram(S=...)``: the Slaney filterbank applied to a given
+    [n_freqs, n_frames] spectrogram (python/metalmom/feature.py:50-57, which
+    multiplies the ``_mel_fb.py`` filterbank into S), in float64."""
+    return mel_filterbank(sr, n_fft, n_mels, fmin, fmax) @ np.asarray(S, np.float64)
+
+
+def dct_ortho(S, n_out):
+    """``mfcc(S=...)``: DCT-II ortho along axis 0 of [n_rows, n_frames], first
+    ``n_out`` rows (feature.py:130-134, scipy ``dct(type=2, norm='ortho')``)."""
+    S = np.asarray(S, np.float64)
+    k = min(n_out, S.shape[0])
+    return dct_basis(k, S.shape[0]) @ S
+
+
 # ---------------------------------------------------------------------------
 # Widening of the path: onset strength, iSTFT, delta, stack_memory
 # ---------------------------------------------------------------------------

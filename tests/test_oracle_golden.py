@@ -182,3 +182,19 @@ def test_istft_inverts_the_oracle_stft():
         np.testing.assert_allclose(r, y, atol=1e-9)
         r2 = O.istft(S, n_fft // 4, center=True)
         assert len(r2) == (S.shape[1] - 1) * (n_fft // 4)
+
+
+def test_mel_project_and_dct_ortho_goldens():
+    """The S= paths (feature.py:50-57, 130-134): the filterbank applied to the
+    power spectrogram gives the mel golden, and the DCT-II ortho of its
+    power_to_db the MFCC golden; the DCT restatement equals scipy's."""
+    from scipy.fftpack import dct
+    y = signal_440()
+    P = O.stft_power(y, 2048, 512, 2048, True)
+    mel = O.mel_project(P, SR, 2048, 128)
+    np.testing.assert_allclose(mel, golden("mel_spectrogram_440hz_default"), rtol=1e-4, atol=1e-4)
+    C = O.dct_ortho(O.power_to_db(mel), 20)
+    np.testing.assert_allclose(C, golden("mfcc_440hz_default"), rtol=1e-4, atol=1e-4)
+    S = np.random.default_rng(3).standard_normal((40, 9))
+    for n in (13, 40, 60):
+        np.testing.assert_allclose(O.dct_ortho(S, n), dct(S, axis=0, type=2, norm="ortho")[:n], atol=1e-12)

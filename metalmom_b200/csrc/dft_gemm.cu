@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
     float Rprev = 0.0f, Rcur = 0.0f, Fcur = 0.0f, chk = 0.0f, fmax_ = -INFINITY;
     auto emit = [&](int m, float v) {
       if (seg_s[m].y) v = __int_as_float(0x7fc00000);
-      const float val = 10.0f * log10f(vthr(v, a.amin) / a.ref);
+      const float val = db10_frame(v, a.amin, 10.0f * log10f(a.ref));
       if (valid) dst[m] = val;
       fmax_ = fmaxf(fmax_, val);
     };
@@ -480,7 +480,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
       while (cur < nmel) finish_seg();
       if (nmel > 0) emit(nmel - 1, Rprev);
       if (!isfinite(chk)) {  // a non-finite bin: every band of the frame is NaN -> amin
-        const float val = 10.0f * log10f(a.amin / a.ref);
+        const float val = db10_frame(a.amin, a.amin, 10.0f * log10f(a.ref));
         if (valid)
           for (int m = 0; m < nmel; m++) dst[m] = val;
         fmax_ = val;

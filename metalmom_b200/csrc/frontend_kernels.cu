@@ -406,7 +406,7 @@ frontend_kernel(FrontArgs a) {
       float *dst = a.out + (cd.frame_off + t) * (long long)a.n_mels;
       for (int m = j; m < a.n_mels; m += TPF) {
         const float acc = mel_dot(mel_s[m], melw, P, bad);
-        const float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        const float v = db10_frame(acc, a.amin, 10.0f * log10f(a.ref));
         if (valid) dst[m] = v;
         vmax = fmaxf(vmax, v);
       }
@@ -542,7 +542,7 @@ __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_f
         const int tt = t0 + fi;
         if (tt >= cd.n_frames) continue;
         const float acc = mel_dot(mel_s[m], melw, P_s + fi * PST, bad_s[fi] != 0);
-        const float v = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        const float v = db10_frame(acc, a.amin, 10.0f * log10f(a.ref));
         a.out[(cd.frame_off + tt) * (long long)a.n_mels + m] = v;
         vmax = fmaxf(vmax, v);
       }

@@ -230,6 +230,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nmel = a.n_mels;
+  const float ref_db = 10.0f * log10f(a.ref);
   // Lane walk over the per-bin split of the filterbank (else packed rows).
   const bool lanes = a.mel_lane_ok != 0;
   const bool mel_in_smem = a.mel_nnz <= kMelSmemMax;
@@ -516,7 +517,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         }
         acc *= 0.25f;
         if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
-        const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        const float val = db10_frame(acc, a.amin, ref_db);
         if (valid) {
           dst[m] = val;
           vmax = fmaxf(vmax, val);
@@ -525,7 +526,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     } else {
       for (int m = l; m < nmel; m += TPF) {
         const float acc = 0.25f * mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
-        const float val = 10.0f * log10f(vthr(acc, a.amin) / a.ref);
+        const float val = db10_frame(acc, a.amin, ref_db);
         if (valid) {
           dst[m] = val;
           vmax = fmaxf(vmax, val);

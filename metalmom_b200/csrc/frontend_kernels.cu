@@ -1351,6 +1351,142 @@ __global__ void __launch_bounds__(256, 3) dct_rows_kernel(DctArgs a) {
   }
 }
 
+// The same whole-row product, software-pipelined (n_mels <= 128): while a
+// tile is multiplied out of shared memory, each thread already holds its part
+// of the next tile's rows in registers (at most 8 float4: 64 frames x n_mels/4
+// float4 over 256 threads), so the HBM latency of the next tile overlaps the
+// arithmetic of this one.  The rows are floored at the clip's threshold on the
+// way into shared memory, as in dct_rows_kernel.
+constexpr int kDctPipeVec = 8;  // float4 per thread and tile (n_mels <= 128)
+
+struct DctTileMeta {
+  long long out_off, T;
+  const float4 *src;
+  int tf, nt;
+  float thr;
+};
+
+__device__ __forceinline__ DctTileMeta dct_tile_meta(const DctArgs &a, int ti) {
+  DctTileMeta m;
+  const int c = __ldg(a.tile_clip + ti);
+  const ClipDesc cd = load_clip(a.clips + c);
+  m.tf = __ldg(a.tile_first + ti);
+  m.nt = min(kDctTile, cd.n_frames - m.tf);
+  m.thr = a.top_db > 0.0f ? dec_f(__ldg(a.clip_max + c)) - a.top_db : -INFINITY;
+  m.src = reinterpret_cast<const float4 *>(a.mel_db + (cd.frame_off + m.tf) * (long long)a.n_mels);
+  m.out_off = cd.out_off;
+  m.T = cd.n_frames;
+  return m;
+}
+
+// NM > 0: n_mels fixed at compile time (the product unrolls with immediate
+// shared-memory offsets); NM == 0: any n_mels <= 128.
+template <int KQ, int NM>
+__global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
+  extern __shared__ __align__(16) float dsm[];
+  const int nm = NM > 0 ? NM : a.n_mels, stride = dct_row_stride(nm), n4 = nm / 4, cnt = kDctTile * n4;
+  float *bas = dsm;                 // [4*KQ][nm]
+  float *tile = dsm + 4 * KQ * nm;  // [64][stride]
+  const int tid = threadIdx.x;
+  const int fr = tid & (kDctTile - 1), kg = tid / kDctTile;
+  for (int i = tid; i < 4 * KQ * nm; i += 256) {
+    const int k = i / nm;
+    bas[i] = k < a.n_mfcc ? __ldg(a.basis + i) : 0.0f;
+  }
+  const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * nm);
+  const float4 *trow = reinterpret_cast<const float4 *>(tile + fr * stride);
+  int ti = blockIdx.x;
+  if (ti >= a.total_tiles) return;
+  float4 pre[kDctPipeVec];
+  DctTileMeta cur = dct_tile_meta(a, ti);
+#pragma unroll
+  for (int v = 0; v < kDctPipeVec; v++) {
+    const int i = tid + 256 * v;
+    pre[v] = (i < cnt && i / n4 < cur.nt) ? __ldg(cur.src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  for (; ti < a.total_tiles; ti += gridDim.x) {
+    __syncthreads();  // every thread is done with the previous tile in shared memory
+#pragma unroll
+    for (int v = 0; v < kDctPipeVec; v++) {
+      const int i = tid + 256 * v;
+      if (i < cnt) {
+        const int r = i / n4, c4 = i - r * n4;
+        float4 x = pre[v];
+        if (r < cur.nt) {
+          x.x = vthr(x.x, cur.thr);
+          x.y = vthr(x.y, cur.thr);
+          x.z = vthr(x.z, cur.thr);
+          x.w = vthr(x.w, cur.thr);
+        }
+        *reinterpret_cast<float4 *>(tile + r * stride + 4 * c4) = x;
+      }
+    }
+    __syncthreads();
+    // next tile's rows into registers while this one is multiplied
+    const int nti = ti + gridDim.x;
+    DctTileMeta nxt = cur;
+    if (nti < a.total_tiles) {
+      nxt = dct_tile_meta(a, nti);
+#pragma unroll
+      for (int v = 0; v < kDctPipeVec; v++) {
+        const int i = tid + 256 * v;
+        pre[v] = (i < cnt && i / n4 < nxt.nt) ? __ldg(nxt.src + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    float acc[KQ];
+#pragma unroll
+    for (int q = 0; q < KQ; q++) acc[q] = 0.0f;
+    if constexpr (NM > 0) {
+#pragma unroll
+      for (int j = 0; j < NM / 4; j++) {
+        const float4 d = trow[j];
+#pragma unroll
+        for (int q = 0; q < KQ; q++) {
+          const float4 b = brow[q * (NM / 4) + j];
+          acc[q] = fmaf(b.x, d.x, acc[q]);
+          acc[q] = fmaf(b.y, d.y, acc[q]);
+          acc[q] = fmaf(b.z, d.z, acc[q]);
+          acc[q] = fmaf(b.w, d.w, acc[q]);
+        }
+      }
+    } else {
+#pragma unroll 2
+      for (int j = 0; j < n4; j++) {
+        const float4 d = trow[j];
+#pragma unroll
+        for (int q = 0; q < KQ; q++) {
+          const float4 b = brow[q * n4 + j];
+          acc[q] = fmaf(b.x, d.x, acc[q]);
+          acc[q] = fmaf(b.y, d.y, acc[q]);
+          acc[q] = fmaf(b.z, d.z, acc[q]);
+          acc[q] = fmaf(b.w, d.w, acc[q]);
+        }
+      }
+    }
+    if (fr < cur.nt) {
+#pragma unroll
+      for (int q = 0; q < KQ; q++) {
+        const int k = kg * KQ + q;
+        if (k < a.n_mfcc) a.out[cur.out_off + (long long)k * cur.T + cur.tf + fr] = acc[q];
+      }
+    }
+    cur = nxt;
+  }
+}
+
+template <int KQ>
+static cudaError_t launch_dct_pipe_t(const DctArgs &a, cudaStream_t s) {
+  const size_t smem = sizeof(float) * ((size_t)4 * KQ * a.n_mels + (size_t)kDctTile * dct_row_stride(a.n_mels));
+  auto kern = a.n_mels == 128 ? dct_pipe_kernel<KQ, 128> : dct_pipe_kernel<KQ, 0>;
+  int per_sm = 1, sms = 148;
+  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(kern), 256, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = (long long)sms * per_sm;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  kern<<<(unsigned)grid, 256, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <int KQ>
 static cudaError_t launch_dct_rows_t(const DctArgs &a, cudaStream_t s) {
   const size_t smem = sizeof(float) * ((size_t)4 * KQ * a.n_mels + (size_t)kDctTile * dct_row_stride(a.n_mels));
@@ -1377,6 +1513,18 @@ cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
   // 4 coefficient groups x KQ accumulators cover min(n_mfcc, 32) coefficients per pass
   const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
+  if (a.n_mfcc <= kDctKC && a.n_mels % 4 == 0 && a.n_mels <= 4 * kDctPipeVec * 256 / kDctTile) {
+    switch (kq) {
+      case 1: return launch_dct_pipe_t<1>(a, s);
+      case 2: return launch_dct_pipe_t<2>(a, s);
+      case 3: return launch_dct_pipe_t<3>(a, s);
+      case 4: return launch_dct_pipe_t<4>(a, s);
+      case 5: return launch_dct_pipe_t<5>(a, s);
+      case 6: return launch_dct_pipe_t<6>(a, s);
+      case 7: return launch_dct_pipe_t<7>(a, s);
+      default: return launch_dct_pipe_t<8>(a, s);
+    }
+  }
   if (a.n_mfcc <= kDctKC && a.n_mels % 4 == 0 && a.n_mels <= 256) {
     switch (kq) {
       case 1: return launch_dct_rows_t<1>(a, s);

@@ -44,6 +44,40 @@ CLIP_SAMPLES = 661500
 N_CLIPS = 256
 
 
+def copy_probe(h2d_bytes, d2h_bytes, stream, chunk, reps=3):
+    """Plain pinned-host <-> device copies of the end-to-end leg's bytes (one
+    contiguous buffer each way, CUDA events): the PCIe bound of the e2e number."""
+    import torch
+    src = torch.empty(h2d_bytes // 4, dtype=torch.float32).pin_memory()
+    dst = torch.empty(h2d_bytes // 4, dtype=torch.float32, device="cuda")
+    back = torch.empty(d2h_bytes // 4, dtype=torch.float32).pin_memory()
+    res = {}
+    with torch.cuda.stream(stream):
+        chunks = [(dst[i:i + chunk // 4], src[i:i + chunk // 4]) for i in range(0, h2d_bytes // 4, chunk // 4)]
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for a, b in chunks:
+            a.copy_(b, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res["h2d_per_clip_copies_gbs"] = h2d_bytes / (e0.elapsed_time(e1) / 1e3) / 1e9
+        for name, a, b, n in (("h2d", dst, src, h2d_bytes), ("d2h", back, dst[: d2h_bytes // 4], d2h_bytes)):
+            a.copy_(b, non_blocking=True)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                a.copy_(b, non_blocking=True)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res[name + "_gbs"] = n * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del src, dst, back
+    res["bound_s"] = h2d_bytes / (res["h2d_gbs"] * 1e9) + d2h_bytes / (res["d2h_gbs"] * 1e9)
+    res["what"] = ("one pinned H2D copy of the step's input bytes plus one D2H copy of its output bytes, "
+                   "back to back; bound_value = audio-hours per step / their summed time")
+    return res
+
+
 def workload_config(n_clips):
     return {
         "workload": f"{n_clips} clips x 30 s @22050 Hz, n_fft 2048, hop 512, 128 mels, 20 MFCC",
@@ -421,10 +455,13 @@ def run_ours(args, rank, world, local_rank):
 
     # pinned host buffers for the end-to-end leg, which runs through a plan cut
     # into branches so that one branch's copies overlap another's kernels
-    pin_in = [torch.from_numpy(c).pin_memory() for c in clips]
-    in_np = [t.numpy() for t in pin_in]
-    pin_out = [torch.empty((plan.rows, f), dtype=torch.float32).pin_memory() for f in plan.frames]
-    out_np = [t.numpy() for t in pin_out]
+    # (one pinned [n_clips, samples] array and one [n_clips, rows, frames]
+    # array, passed as per-clip row views, as a caller holding a batch does)
+    pin_in = torch.from_numpy(np.stack(clips)).pin_memory()
+    in_np = list(pin_in.numpy())
+    pin_out = torch.empty((n_clips, plan.rows, plan.frames[0]), dtype=torch.float32).pin_memory()
+    out_np = list(pin_out.numpy())
+    assert all(f == plan.frames[0] for f in plan.frames)
     plan_io = M.Plan(lengths, clip_params=[dict(sr=SR, n_fft=N_FFT, hop_length=HOP, n_mels=N_MELS,
                                                 n_mfcc=N_MFCC)] * n_clips,
                      max_clips_per_branch=args.e2e_branch_clips)
@@ -477,6 +514,7 @@ def run_ours(args, rank, world, local_rank):
     e2e_value = hours_per_step * world / (e_ms / ke / 1e3)
     h2d = sum(c.nbytes for c in in_np)
     d2h = sum(o.nbytes for o in out_np)
+    copy = copy_probe(h2d, d2h, stream, in_np[0].nbytes) if rank == 0 else None
 
     # ---- the plain one-clip-per-launch GPU form, for comparison
     per_clip = None
@@ -550,7 +588,9 @@ def run_ours(args, rank, world, local_rank):
                          "fp32_fft_tflops": flops_fft / (frame_ms / 1e3) / 1e12},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ke, "branches": plan_io.branches,
-                    "api": "Plan.execute_host (mm_plan_execute_host), pinned host buffers"},
+                    "api": "Plan.execute_host (mm_plan_execute_host), pinned host buffers",
+                    "copy_roofline": dict(copy, bound_value=hours_per_step / copy["bound_s"],
+                                          frac=e2e_value / (hours_per_step / copy["bound_s"]))},
             "clocks": clk.summary(),
             "gpu_launches": K * plan.kernel_launches,
             "one_clip_per_launch": per_clip,

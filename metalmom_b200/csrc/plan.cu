@@ -34,6 +34,7 @@ struct Sub {
   std::vector<int> clips;  // plan clip index of each local clip
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
+  cudaEvent_t in_done = nullptr;  // execute_host: this sub-batch's inputs have landed
   cudaGraph_t graph = nullptr;  // this sub-batch's launches alone
   cudaGraphExec_t exec = nullptr;
   int launches = 0;
@@ -60,6 +61,7 @@ void plan_free(Plan *p) {
     if (s.exec) cudaGraphExecDestroy(s.exec);
     if (s.graph) cudaGraphDestroy(s.graph);
     if (s.done) cudaEventDestroy(s.done);
+    if (s.in_done) cudaEventDestroy(s.in_done);
     if (s.stream) cudaStreamDestroy(s.stream);
   }
   if (p->exec) cudaGraphExecDestroy(p->exec);
@@ -126,6 +128,7 @@ Plan *plan_build(const std::vector<Group> &groups, const std::vector<int> &group
     if (e != cudaSuccess) break;
     e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s.in_done, cudaEventDisableTiming);
     if (e != cudaSuccess) break;
     char *arena = p->base + s.arena_off;
     const size_t desc = carve_arena(s.g, s.L, arena, s.b);
@@ -332,22 +335,44 @@ int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *c
   if (!p || !signals || !outs) return MM_ERR_INVALID_INPUT;
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : p->stream;
   cudaError_t e = cudaEventRecord(p->fork, s);
+  // The uploads are chained in branch order (each branch's copies start when
+  // the previous branch's have landed), so the host link carries one branch
+  // at a time and branch i's kernels run while branch i+1 uploads; issued
+  // side by side, the branches would share the link and land together.
+  cudaEvent_t prev = p->fork;
   for (Sub &b : p->subs) {
     if (e != cudaSuccess) break;
-    e = cudaStreamWaitEvent(b.stream, p->fork, 0);
-    for (size_t k = 0; k < b.clips.size() && e == cudaSuccess; k++) {
+    e = cudaStreamWaitEvent(b.stream, prev, 0);
+    // one copy per run of clips whose host buffers follow each other and whose
+    // device slots do too (e.g. the rows of one [n, length] host array): each
+    // copy carries a fixed cost, so hundreds of per-clip copies cost link time
+    const size_t n = b.clips.size();
+    for (size_t k = 0; k < n && e == cudaSuccess;) {
       const ClipDesc &c = b.L.clips[k];
-      e = cudaMemcpyAsync(b.b.signal + c.sig_off, signals[b.clips[k]], sizeof(float) * (size_t)c.length,
-                          cudaMemcpyHostToDevice, b.stream);
+      const float *h = signals[b.clips[k]];
+      size_t len = (size_t)c.length, j = k + 1;
+      while (j < n && signals[b.clips[j]] == h + len && b.L.clips[j].sig_off == c.sig_off + (long long)len) {
+        len += (size_t)b.L.clips[j].length;
+        j++;
+      }
+      e = cudaMemcpyAsync(b.b.signal + c.sig_off, h, sizeof(float) * len, cudaMemcpyHostToDevice, b.stream);
+      k = j;
     }
+    if (e == cudaSuccess) e = cudaEventRecord(b.in_done, b.stream);
+    prev = b.in_done;
     if (e == cudaSuccess) e = cudaGraphLaunch(b.exec, b.stream);
     const int rows = output_rows(b.g);
-    for (size_t k = 0; k < b.clips.size() && e == cudaSuccess; k++) {
+    for (size_t k = 0; k < n && e == cudaSuccess;) {
       const ClipDesc &c = b.L.clips[k];
-      const size_t cnt = (size_t)rows * (size_t)c.n_frames;
+      float *h = outs[b.clips[k]];
+      size_t cnt = (size_t)rows * (size_t)c.n_frames, j = k + 1;
+      while (j < n && outs[b.clips[j]] == h + cnt && b.L.clips[j].out_off == c.out_off + (long long)cnt) {
+        cnt += (size_t)rows * (size_t)b.L.clips[j].n_frames;
+        j++;
+      }
       if (cnt)
-        e = cudaMemcpyAsync(outs[b.clips[k]], b.b.out + c.out_off, sizeof(float) * cnt, cudaMemcpyDeviceToHost,
-                            b.stream);
+        e = cudaMemcpyAsync(h, b.b.out + c.out_off, sizeof(float) * cnt, cudaMemcpyDeviceToHost, b.stream);
+      k = j;
     }
     if (e == cudaSuccess) e = cudaEventRecord(b.done, b.stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b.done, 0);

@@ -401,3 +401,23 @@ def test_autotune_picks_a_variant_and_keeps_parity():
     y = synth.music_clip(22050 * 4, SR, seed=9)
     got = M.mfcc(y, sr=SR)
     assert O.mfcc_rel_error(got, O.mfcc(y, SR, 20, 2048, 512, 2048, 128)) < MFCC_TOL
+
+
+@pytest.mark.parametrize("length", [22048, 22051])
+def test_plan_host_io_from_one_batch_array(length):
+    """Clips passed as rows of one host array (their buffers adjacent) are
+    uploaded and downloaded as merged runs; the results equal those from
+    separate buffers bitwise.  Length 22051 leaves a 4-float alignment gap
+    between the device slots, so no run forms there."""
+    n = 12
+    batch = np.stack([synth.music_clip(length, SR, seed=900 + i) for i in range(n)])
+    sep = [row.copy() for row in batch]
+    with M.Plan([length] * n, clip_params=[dict(sr=SR, n_fft=2048, hop_length=512)] * n,
+                max_clips_per_branch=5) as plan:
+        assert plan.branches == 3
+        ref = plan.execute_host(sep)
+        out = np.empty((n,) + ref[0].shape, np.float32)
+        got = plan.execute_host(list(batch), list(out))
+    for i in range(n):
+        np.testing.assert_array_equal(got[i], ref[i])
+        np.testing.assert_array_equal(out[i], ref[i])

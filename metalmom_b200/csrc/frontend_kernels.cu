@@ -901,7 +901,8 @@ __global__ void build_mel_seg_kernel(int2 *seg, const int *bin_seg, const int4 *
 //   band[m]          = first slot of segment m | count(m) << 12 |
 //                      count(m+1) << 18 | NaN flag of band m << 24
 // band m = sum of .x over its own parts + sum of .y over the parts of m+1.
-// ok[2] = 1 when the split holds and the parts fit in `max_slots`.
+// ok[2] = 1 when the split holds, every weight is finite and the parts fit in
+// `max_slots`.
 __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const float2 *w2, const int *bin_seg,
                                       const int2 *seg, int n_mels, int tpf, int max_slots, int *ok) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
@@ -920,6 +921,7 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
     for (int b = 0; b <= last; b++) {
       const int k = 32 * l + b;
       sid = next_sid(k, sid);
+      if (!isfinite(w2[k].x) || !isfinite(w2[k].y)) return;  // the walk's check needs finite weights
       lw[b * tpf + l] = w2[k];
       const bool flush = (b == last) || next_sid(k + 1, sid) != sid;
       if (!flush) continue;

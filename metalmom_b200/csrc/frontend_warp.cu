@@ -176,10 +176,18 @@ struct WShape {
   static_assert(TPF >= 4 && TPF <= 32, "n_fft must be 256..2048");
 };
 
+// Real-split twiddles W_N^(l + 32 i), i < 16, of lane l (one frame per warp
+// only): 512 complex, read as [32 i + l].
+template <int LOG2N>
+__host__ __device__ constexpr size_t warp_split_tw() {
+  return WShape<LOG2N>::C == 1 ? size_t(16 * 32) * 8 : 0;
+}
+
 template <int LOG2N>
 __host__ __device__ constexpr size_t warp_fixed_smem() {
   using S = WShape<LOG2N>;
-  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + size_t(S::F) * S::FSTRIDE * 8;
+  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + warp_split_tw<LOG2N>() +
+         size_t(S::F) * S::FSTRIDE * 8;
 }
 
 int warp_frames_per_tile(int log2n) {
@@ -239,6 +247,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   sp += align16(size_t(31) * TPF * 8);
   float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
   sp += align16(size_t(N) * 4);
+  cpx *rs_tw = reinterpret_cast<cpx *>(sp);  // C == 1: real-split twiddles [32 i + l]
+  sp += warp_split_tw<LOG2N>();
   cpx *bufs = reinterpret_cast<cpx *>(sp);
   sp += size_t(F) * S::FSTRIDE * 8;
   // lanes: band words, lane words, lane-minor weights; else packed rows
@@ -259,6 +269,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   }
   for (int i = tid; i < N / 4; i += S::THREADS)
     reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+  if constexpr (C == 1)
+    for (int i = tid; i < 16 * 32; i += S::THREADS) rs_tw[i] = root_q(twq, (i & 31) + 32 * (i >> 5), N);
   if (lanes) {
     for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
     for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
@@ -386,7 +398,6 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     __syncwarp();  // every lane has read its columns: fb becomes P
 
     // ---- real split, P[k] = |2 X[k]|^2
-    float chk = 0.0f;
     if constexpr (C == 1) {
       // lanes l and 32-l swap registers 16..31: pair i of lane l is
       // (Z[l + 32 i], Z[M - l - 32 i]) = (v[i], partner's v[31 - i]); lane 0
@@ -409,7 +420,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         else zb = l0 ? rcv[16 - i] : rcv[15 - i];
         const float ex = za.x + zb.x, ey = za.y - zb.y;
         const float ox = za.y + zb.y, oy = zb.x - za.x;
-        const cpx w = tw_const<i, 64>(base_c[0]);
+        const cpx w = rs_tw[32 * i + l];  // W_N^(l + 32 i)
         const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
         const float xr = ex + wr, xi = ey + wi;
         const float yr = ex - wr, yi = ey - wi;
@@ -417,13 +428,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         Pa[33 * i] = p;
         if constexpr (i == 0) Pb[l0 ? -1 : 0] = q;  // lane 0: the Nyquist bin
         else Pb[-33 * i] = q;
-        chk += p + q;
       });
-      if (l0) {
-        const float p = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
-        P[M / 2 + TPF / 2] = p;
-        chk += p;
-      }
+      if (l0) P[M / 2 + TPF / 2] = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
     } else {
       const bool l0 = (l == 0);
       static_for<0, HALF>([&](auto ci) {
@@ -462,17 +468,13 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
             P[ka + k2] = p;
             P[M - ka + TPF - 1 - k2] = q;
           }
-          chk += p + q;
         });
       });
       if (l0) {
         const cpx zm = v[TPF / 2];
-        const float p = 4.0f * fmaf(zm.x, zm.x, zm.y * zm.y);
-        P[M / 2 + TPF / 2] = p;
-        chk += p;
+        P[M / 2 + TPF / 2] = 4.0f * fmaf(zm.x, zm.x, zm.y * zm.y);
       }
     }
-    const bool bad = (__ballot_sync(FULL, !isfinite(chk)) & gmask) != 0;
     __syncwarp();  // P complete
 
     // ---- log-mel row of this frame + running clip max
@@ -488,7 +490,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       int slot = li.y;
       const float *pl = P + 33 * l;
       const float2 *wl = lw_s + l;
-      float R = 0.0f, Fs = 0.0f;
+      // Every bin enters both sums (zero weights included; the lane tables
+      // hold finite weights only), so a non-finite bin makes its part
+      // non-finite: `tot` over the parts carries the frame's check.
+      float R = 0.0f, Fs = 0.0f, tot = 0.0f;
 #pragma unroll
       for (int b = 0; b < 32; b++) {
         const float p = pl[b];
@@ -497,6 +502,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         Fs = fmaf(w.y, p, Fs);
         if (fl & (1u << b)) {
           parts[slot++] = make_float2(R, Fs);
+          tot += R + Fs;
           R = 0.0f;
           Fs = 0.0f;
         }
@@ -504,8 +510,12 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       if (l == TPF - 1) {
         const float p = pl[32];
         const float2 w = wl[32 * TPF];
-        parts[slot] = make_float2(fmaf(w.x, p, R), fmaf(w.y, p, Fs));
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        parts[slot] = make_float2(R, Fs);
+        tot += R + Fs;
       }
+      const bool bad = (__ballot_sync(FULL, !isfinite(tot)) & gmask) != 0;
       __syncwarp();
       for (int m = l; m < nmel; m += TPF) {
         const int bw = band_s[m];
@@ -524,6 +534,9 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         }
       }
     } else {
+      float chk = 0.0f;  // the frame's non-finite check: this lane's share of the bins
+      for (int k = l; k <= M; k += TPF) chk += P[pad_bin<TPF>(k)];
+      const bool bad = (__ballot_sync(FULL, !isfinite(chk)) & gmask) != 0;
       for (int m = l; m < nmel; m += TPF) {
         const float acc = 0.25f * mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
         const float val = db10_frame(acc, a.amin, ref_db);

@@ -421,3 +421,21 @@ def test_plan_host_io_from_one_batch_array(length):
     for i in range(n):
         np.testing.assert_array_equal(got[i], ref[i])
         np.testing.assert_array_equal(out[i], ref[i])
+
+
+@pytest.mark.parametrize("n_fft,hop,n_mels", [(2048, 512, 128), (512, 128, 120)])
+def test_nonfinite_samples_floor_their_frames(n_fft, hop, n_mels):
+    """A NaN or an infinite sample makes every band of the frames that hold it
+    non-finite, which vDSP_vthr maps to amin (-100 dB) before the top_db floor;
+    the other frames are untouched.  (2048, 128): the lane walk's check;
+    (512, 120): too many filterbank parts for the lane tables, so the packed
+    rows and their own check.)"""
+    y = synth.music_clip(22050, SR, seed=31)
+    y[5000] = np.nan
+    y[15000] = np.inf
+    y[18000] = -np.inf
+    with np.errstate(all="ignore"):
+        exp = O.mfcc(y, SR, 20, n_fft, hop, n_fft, n_mels)
+    got = M.mfcc(y, sr=SR, n_fft=n_fft, hop_length=hop, n_mels=n_mels)
+    assert got.shape == exp.shape and np.isfinite(got).all()
+    assert O.mfcc_rel_error(got, exp) < MFCC_TOL

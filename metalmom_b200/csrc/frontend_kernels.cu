@@ -894,26 +894,29 @@ __global__ void build_mel_seg_kernel(int2 *seg, const int *bin_seg, const int4 *
 // M = 32 tpf); it accumulates (R, F) = sum of (w2.x P, w2.y P) and stores the
 // pair in the next "part" slot wherever the segment of bin k differs from that
 // of bin k+1, and after its last bin.  Parts are numbered lane after lane, so
-// the pieces of segment s occupy consecutive slots and segment s+1 starts where
-// s ends.
+// the pieces of a segment occupy consecutive slots: its head (the first) and
+// the first parts of the following lanes it runs into.  After the walk the
+// lane holding a head adds those k continuation parts into it, so each
+// segment's sums sit in its head slot and band m = head(m).x + head(m+1).y.
 //   lw[b * tpf + l]  = w2[32 l + b], b <= 32 (b = 32: Nyquist, last lane only)
-//   lane[l]          = {flush mask over b < 32, first slot of lane l}
-//   band[m]          = first slot of segment m | count(m) << 12 |
-//                      count(m+1) << 18 | NaN flag of band m << 24
-// band m = sum of .x over its own parts + sum of .y over the parts of m+1.
-// ok[2] = 1 when the split holds, every weight is finite and the parts fit in
-// `max_slots`.
+//   lane[l]          = {flush mask over b < 32,
+//                       first slot of lane l | k << 10 | zero slot << 16}
+//   band[m]          = head slot of segment m | head slot of m+1 << 12 |
+//                      NaN flag of band m << 24   (an empty segment: the zero
+//                      slot, which the kernel clears every frame)
+// ok[2] = 1 when the split holds, every weight is finite and the parts and the
+// zero slot fit in `max_slots`.
 __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const float2 *w2, const int *bin_seg,
                                       const int2 *seg, int n_mels, int tpf, int max_slots, int *ok) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   ok[2] = 0;
-  if (!ok[1]) return;
-  for (int m = 0; m < n_mels; m++) band[m] = 0;
+  if (!ok[1] || tpf > 32) return;
+  for (int m = 0; m < n_mels; m++) band[m] = 0;  // first(s) | count(s) << 12 during the walk
   int slot = 0, sid = -1;
+  int last_slot[32], last_sid[32];
   // segment of bin k: the band of the last bin at or below k that feeds one
   // (bins with no band carry on the run before them, with zero weights)
   auto next_sid = [&](int k, int cur) { return bin_seg[k] >= 0 ? bin_seg[k] : cur; };
-  // first(s) accumulates in the low 12 bits of band[s], count(s) in bits 12..17
   for (int l = 0; l < tpf; l++) {
     lane[l] = make_int2(0, slot);
     const int last = (l == tpf - 1) ? 32 : 31;
@@ -927,28 +930,31 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
       if (!flush) continue;
       if (b < 32) mask |= 1u << b;
       if (sid >= 0) {
-        if (slot >= 4096 || sid >= n_mels) return;
+        if (slot >= 1023 || sid >= n_mels) return;
         int w = band[sid];
         if (((w >> 12) & 63) == 0) w = slot;  // first part of segment sid
         w += 1 << 12;
         band[sid] = w;
       }
+      last_slot[l] = slot;
+      last_sid[l] = sid;
       slot++;
     }
     if (l < tpf - 1) lw[32 * tpf + l] = make_float2(0.0f, 0.0f);
     lane[l].x = (int)mask;
   }
-  if (slot > max_slots) return;
-  // empty segments start where the next one does; then add count(m+1) and the
-  // NaN flag
-  int next_first = slot;
-  for (int m = n_mels - 1; m >= 0; m--) {
-    if (((band[m] >> 12) & 63) == 0) band[m] = next_first;
-    next_first = band[m] & 4095;
+  const int zero = slot;
+  if (zero + 1 > max_slots) return;
+  for (int l = 0; l < tpf; l++) {
+    const int s = last_sid[l];
+    int k = 0;
+    if (s >= 0 && last_slot[l] == (band[s] & 4095)) k = ((band[s] >> 12) & 63) - 1;  // lane l holds the head
+    lane[l].y |= (k << 10) | (zero << 16);
   }
-  for (int m = 0; m < n_mels; m++) {
-    const int cnt_next = (m + 1 < n_mels) ? ((band[m + 1] >> 12) & 63) : 0;
-    band[m] |= (cnt_next << 18) | ((seg[m].y ? 1 : 0) << 24);
+  for (int m = 0; m < n_mels; m++) {  // band[m + 1] is still in the walk's form when band[m] is rewritten
+    const int hr = ((band[m] >> 12) & 63) ? (band[m] & 4095) : zero;
+    const int hf = (m + 1 < n_mels && ((band[m + 1] >> 12) & 63)) ? (band[m + 1] & 4095) : zero;
+    band[m] = hr | (hf << 12) | ((seg[m].y ? 1 : 0) << 24);
   }
   ok[2] = 1;
 }

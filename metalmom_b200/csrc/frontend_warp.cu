@@ -482,12 +482,13 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     if (lanes) {
       // lane l sums its 32 bins (the last lane also the Nyquist bin) into
       // (R, F) = (w.x P, w.y P) and stores the pair in the next part slot at
-      // every segment end; band m then adds the .x of its own parts and the .y
-      // of the parts of segment m + 1 (consecutive slots).
+      // every segment end; the lane holding a segment's head then adds the
+      // parts of the lanes the segment runs into, and band m is the head of
+      // segment m (.x) plus the head of segment m + 1 (.y).
       float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
       const int2 li = lane_s[l];
       const unsigned fl = (unsigned)li.x;
-      int slot = li.y;
+      int slot = li.y & 1023;
       const float *pl = P + 33 * l;
       const float2 *wl = lw_s + l;
       // Every bin enters both sums (zero weights included; the lane tables
@@ -516,15 +517,24 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         tot += R + Fs;
       }
       const bool bad = (__ballot_sync(FULL, !isfinite(tot)) & gmask) != 0;
+      if (l == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);  // the empty segments' slot
+      __syncwarp();
+      // fix-up: this lane's last part heads a segment that runs into the next k lanes
+      const int kc = (li.y >> 10) & 63;
+      if (kc) {
+        const int h = l == TPF - 1 ? slot : slot - 1;
+        float2 hv = parts[h];
+        for (int j = 1; j <= kc; j++) {
+          const float2 pv = parts[h + j];
+          hv.x += pv.x;
+          hv.y += pv.y;
+        }
+        parts[h] = hv;
+      }
       __syncwarp();
       for (int m = l; m < nmel; m += TPF) {
         const int bw = band_s[m];
-        const int first = bw & 4095, cr = (bw >> 12) & 63, cn = cr + ((bw >> 18) & 63);
-        float acc = 0.0f;
-        for (int j = 0; j < cn; j++) {
-          const float2 pv = parts[first + j];
-          acc += j < cr ? pv.x : pv.y;
-        }
+        float acc = parts[bw & 4095].x + parts[(bw >> 12) & 4095].y;
         acc *= 0.25f;
         if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
         const float val = db10_frame(acc, a.amin, ref_db);

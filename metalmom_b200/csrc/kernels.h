@@ -60,8 +60,8 @@ struct DevTables {
   // l of a frame owns bins [32 l, 32 l + 32) and sums them into per-segment
   // parts (layout at build_mel_lane_kernel).
   float2 *mel_lw = nullptr;    // [33][n_fft/64] weights, lane-minor
-  int2 *mel_lane = nullptr;    // per lane {flush mask, first part slot}
-  int *mel_band = nullptr;     // per band: first part | counts | NaN flag
+  int2 *mel_lane = nullptr;    // per lane {flush mask, first slot | chain length | zero slot}
+  int *mel_band = nullptr;     // per band: head slot of m | head slot of m+1 | NaN flag
   int mel_lane_ok = 0;
   // DFT-as-GEMM form only: the windowed DFT basis as bf16 hi/lo images and an
   // error word the kernel sets when a bounded wait runs out.

@@ -439,3 +439,32 @@ def test_nonfinite_samples_floor_their_frames(n_fft, hop, n_mels):
     got = M.mfcc(y, sr=SR, n_fft=n_fft, hop_length=hop, n_mels=n_mels)
     assert got.shape == exp.shape and np.isfinite(got).all()
     assert O.mfcc_rel_error(got, exp) < MFCC_TOL
+
+
+@pytest.mark.parametrize("n_fft,n_mels,fmin,fmax", [
+    (2048, 1, 0.0, None),        # one band: its segment runs through every lane
+    (2048, 20, 0.0, None),       # wide bands: segments over several lanes
+    (2048, 64, 300.0, 4000.0),   # bins past fmax carry the last segment to the end
+    (2048, 256, 0.0, None),
+    (1024, 64, 0.0, None),
+    (512, 100, 0.0, None),       # lane tables near their slot limit
+    (512, 120, 0.0, None),       # over it: packed rows
+    (256, 40, 50.0, None),
+])
+def test_warp_kernel_filterbank_shapes_vs_oracle(n_fft, n_mels, fmin, fmax):
+    """The warp kernel's filterbank walk (parts per lane, segment heads that
+    take the parts of the lanes they run into, two-slot bands) on filterbanks
+    that stress its tables; n_mfcc = n_mels where the DCT allows it, so the
+    MFCC bound also bounds the log-mel rows."""
+    y = synth.music_clip(4 * SR + 77, SR, seed=n_fft + n_mels)
+    n_mfcc = min(n_mels, 32)
+    old = M.tune_get(n_fft)
+    try:
+        M.tune_set(n_fft, 3)
+        got = M.mfcc(y, sr=SR, n_mfcc=n_mfcc, n_fft=n_fft, hop_length=n_fft // 4, n_mels=n_mels,
+                     fmin=fmin, fmax=fmax)
+    finally:
+        M.tune_set(n_fft, old)
+    exp = O.mfcc(y, SR, n_mfcc, n_fft, n_fft // 4, n_fft, n_mels, fmin, fmax)
+    assert got.shape == exp.shape
+    assert O.mfcc_rel_error(got, exp) < MFCC_TOL, O.mfcc_rel_error(got, exp)

@@ -14,15 +14,24 @@
 // (v = hi + lo); the BF16x3 form accumulates hi*hi + hi*lo + lo*hi in one
 // float32 TMEM accumulator, the plain BF16 form hi*hi only.
 //
-// Per CTA (128 threads, one frame per thread = one TMEM lane), per N tile of
-// at most 256 columns, per K chunk of 64: the threads write the A chunk (from
-// the signal) and the B chunk (a pre-swizzled image) into shared memory in
-// the K-major 128-byte-swizzle layout, thread 0 issues the tcgen05.mma
-// instructions and commits them to an mbarrier.  After the last chunk each
-// warp reads its 32 lanes of the accumulator (tcgen05.ld), forms |X|^2, and
-// folds the bins into the mel bands with the per-bin split of the filterbank
-// (band m = R[m] + F[m+1]); the log-mel row and the clip maximum are written as
-// by the FFT kernels, and the same DCT kernel follows.
+// One CTA per SM (it holds all 512 TMEM columns), warp-specialised, with
+// mbarriers between the roles instead of block-wide barriers:
+//  * 16 producer warps: four threads per frame row convert 16 samples each of
+//    the K chunk (64 samples) into bf16 hi/lo in the K-major 128-byte-swizzle
+//    layout of the A ring (2 stages), with the samples of the next two chunks
+//    already loading; producer thread 0 also moves each basis chunk (a
+//    pre-swizzled image, hi and lo) into the B ring (3 stages where shared
+//    memory allows, 2 otherwise) by bulk async copies;
+//  * one MMA thread: per chunk 4 (bf16) or 12 (bf16x3) tcgen05.mma of
+//    M 128 x N tile_cols x K 16 into one of two TMEM accumulators, committed
+//    to the stages' "empty" barriers and, after the last chunk of an N tile,
+//    to the accumulator's "full" barrier;
+//  * 4 epilogue warps (TMEM lane quarters): while the next N tile fills the
+//    other accumulator, each thread reads its frame's columns (tcgen05.ld),
+//    forms |X|^2 and folds the bins into the mel bands with the per-bin split
+//    of the filterbank (band m = R[m] + F[m+1]); the log-mel row and the clip
+//    maximum are written as by the FFT kernels, and the same DCT kernel
+//    follows.
 //
 // Every wait is bounded: a wait that runs out sets the error word and the
 // CTA stops, releases its tensor memory and returns.
@@ -39,9 +48,17 @@ namespace mm {
 
 constexpr int kDftM = 128;   // frames per tile = TMEM lanes
 constexpr int kDftKC = 64;   // K per chunk: one 128-byte swizzle row of bf16
-constexpr int kDftThreads = 256;  // 8 warps: two per TMEM lane quarter
-constexpr int kDftTmemCols = 256;
-constexpr size_t kDftMinSmem = 80 * 1024;  // at most two CTAs per SM: 2 x 256 TMEM columns
+// Warp roles: 16 producer warps (four threads per frame row build the A
+// chunk, 16 samples each, two chunks of samples in flight), 4 epilogue warps
+// (warp 16 + q reads TMEM lane quarter q), 1 MMA warp.
+constexpr int kDftRowSplit = 4;
+constexpr int kDftRowCols = kDftKC / kDftRowSplit;  // 16 samples per producer thread
+constexpr int kDftProducers = kDftM * kDftRowSplit;
+constexpr int kDftEpiWarp0 = kDftProducers / 32;
+constexpr int kDftMmaWarp = kDftEpiWarp0 + 4;
+constexpr int kDftThreads = 32 * (kDftMmaWarp + 1);
+constexpr int kDftTmemCols = 512;  // two accumulators of up to 256 columns
+constexpr int kDftAStages = 2;     // A chunks: built on the SM, quickly
 
 DftShape dft_shape(int n_fft, int win) {
   DftShape s{};
@@ -202,16 +219,16 @@ __device__ __forceinline__ void split8(const float *x, uint4 &hi, uint4 &lo) {
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-constexpr int kDftStages = 2;
 
-// 32 samples (x[first + q], q < 32) of one frame row, with the padding rule
+// NS samples (x[first + q], q < NS) of one frame row, with the padding rule
 // of sample_at; zeros for frames past the clip.
-__device__ __forceinline__ void load_row32(float *x, const float *sig, long long first, long long length,
-                                           long long sig_off, int pad_mode, bool valid) {
-  if (valid && first >= 0 && first + 32 <= length && ((sig_off + first) & 3) == 0) {
+template <int NS>
+__device__ __forceinline__ void load_row(float *x, const float *sig, long long first, long long length,
+                                         long long sig_off, int pad_mode, bool valid) {
+  if (valid && first >= 0 && first + NS <= length && ((sig_off + first) & 3) == 0) {
     const float4 *p4 = reinterpret_cast<const float4 *>(sig + first);
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < NS / 4; q++) {
       const float4 v = __ldg(p4 + q);
       x[4 * q] = v.x;
       x[4 * q + 1] = v.y;
@@ -220,35 +237,36 @@ __device__ __forceinline__ void load_row32(float *x, const float *sig, long long
     }
   } else {
 #pragma unroll
-    for (int q = 0; q < 32; q++) x[q] = valid ? sample_at(sig, first + q, length, pad_mode) : 0.0f;
+    for (int q = 0; q < NS; q++) x[q] = valid ? sample_at(sig, first + q, length, pad_mode) : 0.0f;
   }
 }
 
+// Shared memory: the A ring (hi, lo), the B ring (hi, lo: basis chunks by
+// bulk copy; three stages when they fit, to cover the L2 latency), the
+// per-bin filterbank split and the barriers.
 struct DftSmem {
-  size_t a_hi[kDftStages], a_lo[kDftStages], b_hi[kDftStages], b_lo[kDftStages];
-  size_t w2, seg, bar, taddr, total;
+  int b_stages;
+  size_t a0, a_stage, b0, b_stage, b_img, w2, seg, bar, taddr, total;
 };
 __host__ __device__ inline DftSmem dft_smem_layout(const DftShape &s, int n_mels) {
   DftSmem L{};
+  const size_t a_img = (size_t)kDftM * 128;
+  L.b_img = ((size_t)s.tile_cols * 128 + 1023) & ~size_t(1023);
+  L.a_stage = 2 * a_img;
+  L.b_stage = 2 * L.b_img;
+  const size_t tail = align16(8 * (size_t)s.nbins) + align16(8 * (size_t)(n_mels + 1)) + 256 + 1024;
+  L.b_stages = (kDftAStages * L.a_stage + 3 * L.b_stage + tail <= 227 * 1024) ? 3 : 2;
   size_t p = 0;
-  const size_t a_bytes = (size_t)kDftM * 128, b_bytes = ((size_t)s.tile_cols * 128 + 1023) & ~size_t(1023);
-  for (int st = 0; st < kDftStages; st++) {
-    L.a_hi[st] = p;
-    p += a_bytes;
-    L.a_lo[st] = p;
-    p += a_bytes;
-    L.b_hi[st] = p;
-    p += b_bytes;
-    L.b_lo[st] = p;
-    p += b_bytes;
-  }
-  // the power spectrum of one N tile ([bins][128] floats) reuses the stages
+  L.a0 = p;
+  p += kDftAStages * L.a_stage;
+  L.b0 = p;
+  p += (size_t)L.b_stages * L.b_stage;
   L.w2 = p;
   p += align16(8 * (size_t)s.nbins);
   L.seg = p;
   p += align16(8 * (size_t)(n_mels + 1));
-  L.bar = p;  // full[2], empty[2]
-  p += 32;
+  L.bar = p;  // a_full[2] a_empty[2] b_full[3] b_empty[3] acc_full[2] acc_empty[2] fin
+  p += 8 * 16;
   L.taddr = p;
   p += 16;
   L.total = p + 1024;  // slack to align the base to 1024 bytes
@@ -257,6 +275,10 @@ __host__ __device__ inline DftSmem dft_smem_layout(const DftShape &s, int n_mels
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // One arrival that also announces `bytes` of bulk copies completing on the barrier.
@@ -278,28 +300,41 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   const uint32_t raw = smem_u32(smem_raw);
   unsigned char *sm = smem_raw + (((raw + 1023u) & ~1023u) - raw);
   const DftSmem Ly = dft_smem_layout(S, a.n_mels);
-  float *P = reinterpret_cast<float *>(sm);  // [bins of the N tile][128], after its MMAs
+  const int SB = Ly.b_stages;
   float2 *w2_s = reinterpret_cast<float2 *>(sm + Ly.w2);
   int2 *seg_s = reinterpret_cast<int2 *>(sm + Ly.seg);
   const uint32_t bar0 = smem_u32(sm + Ly.bar);
-  auto full_bar = [&](int st) { return bar0 + 8u * (uint32_t)st; };
-  auto empty_bar = [&](int st) { return bar0 + 16u + 8u * (uint32_t)st; };
+  auto a_full = [&](int st) { return bar0 + 8u * (uint32_t)st; };
+  auto a_empty = [&](int st) { return bar0 + 16u + 8u * (uint32_t)st; };
+  auto b_full = [&](int st) { return bar0 + 32u + 8u * (uint32_t)st; };
+  auto b_empty = [&](int st) { return bar0 + 56u + 8u * (uint32_t)st; };
+  auto acc_full = [&](int b) { return bar0 + 80u + 8u * (uint32_t)b; };
+  auto acc_empty = [&](int b) { return bar0 + 96u + 8u * (uint32_t)b; };
+  const uint32_t fin = bar0 + 112u;
   uint32_t *taddr_s = reinterpret_cast<uint32_t *>(sm + Ly.taddr);
+  const uint32_t b_img = (uint32_t)S.tile_cols * 128u;
 
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int row = tid & (kDftM - 1);  // frame of the tile (= TMEM lane)
-  const int half = tid >> 7;          // which 32 columns of a chunk this thread builds
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nmel = a.n_mels;
   for (int i = tid; i < S.nbins; i += kDftThreads) w2_s[i] = __ldg(a.mel_w2 + i);
   for (int i = tid; i <= nmel; i += kDftThreads) seg_s[i] = __ldg(a.mel_seg + i);
   if (tid == 0) {
-    for (int st = 0; st < kDftStages; st++) {
-      mbar_init(full_bar(st), 1);
-      mbar_init(empty_bar(st), 1);
+    for (int st = 0; st < kDftAStages; st++) {
+      mbar_init(a_full(st), kDftProducers);
+      mbar_init(a_empty(st), 1);
     }
+    for (int st = 0; st < SB; st++) {
+      mbar_init(b_full(st), 1);
+      mbar_init(b_empty(st), 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      mbar_init(acc_full(b), 1);
+      mbar_init(acc_empty(b), kDftM);
+    }
+    mbar_init(fin, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == kDftMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
                  "r"(kDftTmemCols)
                  : "memory");
@@ -309,194 +344,212 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *taddr_s;
-  const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const uint32_t idesc = idesc_bf16(S.tile_cols);
-  const uint32_t b_img = (uint32_t)S.tile_cols * 128u;
-  const int seg_lo = seg_s[0].x, seg_hi = seg_s[nmel].x;
-
-  // per-stage state as bits (stage st = bit st): expected phase parities and
-  // whether an MMA commit on empty[st] has not been waited for yet
-  uint32_t full_ph = 0, empty_ph = 0, pend = 0;
-  const size_t stage_stride = Ly.a_hi[1] - Ly.a_hi[0];
-  uint32_t chunk = 0;
-  bool failed = false, broken = false;
-  int cur_clip = -1;
-  float vmax = -INFINITY;
   const int total = a.total_tiles;
   const int t_begin = (int)((long long)blockIdx.x * total / gridDim.x);
   const int t_end = (int)((long long)(blockIdx.x + 1) * total / gridDim.x);
 
-  for (int tile = t_begin; tile < t_end && !failed; tile++) {
-    const int c = __ldg(a.tile_clip + tile);
-    if (c != cur_clip) {
-      float m = vmax;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-      if ((tid & 31) == 0 && cur_clip >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur_clip, enc_f(m));
-      cur_clip = c;
-      vmax = -INFINITY;
-    }
-    const ClipDesc cd = load_clip(a.clips + c);
-    const int t = (tile - cd.tile_base) * kDftM + row;  // this thread's frame
-    const bool valid = t < cd.n_frames;
-    const float *sig = a.signal + cd.sig_off;
-    const long long s0 = (long long)t * a.hop - a.pad + S.k0 + 32 * half;
-    float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
-    // mel state of this frame (threads of half 0), bins arrive in order across N tiles
-    int cur = 0;
-    float Rprev = 0.0f, Rcur = 0.0f, Fcur = 0.0f, chk = 0.0f, fmax_ = -INFINITY;
-    auto emit = [&](int m, float v) {
-      if (seg_s[m].y) v = __int_as_float(0x7fc00000);
-      const float val = db10_frame(v, a.amin, 10.0f * log10f(a.ref));
-      if (valid) dst[m] = val;
-      fmax_ = fmaxf(fmax_, val);
-    };
-    auto finish_seg = [&]() {
-      if (cur >= 1) emit(cur - 1, Rprev + Fcur);
-      Rprev = Rcur;
-      Rcur = 0.0f;
-      Fcur = 0.0f;
-      cur++;
-    };
-
-    // samples of the next K chunk, loaded one chunk ahead (a chunk's samples
-    // are the same for every N tile)
-    float xn[32];
-    load_row32(xn, sig, s0, cd.length, cd.sig_off, a.pad_mode, valid);
-    for (int nt = 0; nt < S.ntiles && !failed; nt++) {
-      for (int kc = 0; kc < S.kchunks; kc++) {
-        const int st = (int)(chunk & 1u);
-        bool ok = true;
-        const uint32_t bit = 1u << st;
-        if (pend & bit) {  // the MMAs that read this stage two chunks ago are done
-          ok = mbar_wait_bounded(empty_bar(st), (empty_ph >> st) & 1u);
-          empty_ph ^= bit;
-          pend &= ~bit;
-        }
-        unsigned char *stage = sm + (size_t)st * stage_stride;
-        unsigned char *a_hi = stage + Ly.a_hi[0], *a_lo = stage + Ly.a_lo[0];
-        unsigned char *b_hi = stage + Ly.b_hi[0], *b_lo = stage + Ly.b_lo[0];
-        if (tid == 0 && ok && !broken) {
-          const char *src = reinterpret_cast<const char *>(basis) + (size_t)(nt * S.kchunks + kc) * 2 * b_img;
-          mbar_expect_tx(full_bar(st), SPLIT == 3 ? 2u * b_img : b_img);
-          bulk_g2s(smem_u32(b_hi), src, b_img, full_bar(st));
-          if (SPLIT == 3) bulk_g2s(smem_u32(b_lo), src + b_img, b_img, full_bar(st));
-        }
-        // ---- A chunk: this thread's 32 samples of its frame row
-        {
-          float x[32];
-#pragma unroll
-          for (int q = 0; q < 32; q++) x[q] = xn[q];
-          const bool last = kc + 1 == S.kchunks && nt + 1 == S.ntiles;
-          if (!last) {
-            const int kn = kc + 1 < S.kchunks ? kc + 1 : 0;
-            load_row32(xn, sig, s0 + (long long)kn * kDftKC, cd.length, cd.sig_off, a.pad_mode, valid);
+  if (warp < kDftEpiWarp0) {
+    // ---------------- producers: A chunks (and thread 0: the basis chunks)
+    const int row = tid & (kDftM - 1), part = tid >> 7;  // 16 columns of the chunk per thread
+    uint32_t c = 0;  // chunk counter (A ring stage c % 2, B ring stage c % SB)
+    bool ok = true;
+    for (int tile = t_begin; tile < t_end && ok; tile++) {
+      const int cl = __ldg(a.tile_clip + tile);
+      const ClipDesc cd = load_clip(a.clips + cl);
+      const int t = (tile - cd.tile_base) * kDftM + row;
+      const bool valid = t < cd.n_frames;
+      const float *sig = a.signal + cd.sig_off;
+      const long long s0 = (long long)t * a.hop - a.pad + S.k0 + kDftRowCols * part;
+      // samples two chunks ahead (a chunk's samples serve every N tile)
+      const int nchunks = S.ntiles * S.kchunks;
+      float xn[kDftRowCols], xn2[kDftRowCols];
+      load_row<kDftRowCols>(xn, sig, s0, cd.length, cd.sig_off, a.pad_mode, valid);
+      load_row<kDftRowCols>(xn2, sig, s0 + (long long)(1 % S.kchunks) * kDftKC, cd.length, cd.sig_off,
+                            a.pad_mode, valid && nchunks > 1);
+      for (int nt = 0; nt < S.ntiles && ok; nt++) {
+        for (int kc = 0; kc < S.kchunks && ok; kc++, c++) {
+          const int sa = (int)(c % kDftAStages), sb = (int)(c % (uint32_t)SB);
+          const uint32_t pa = (c / kDftAStages) & 1u, pb = (c / (uint32_t)SB) & 1u;
+          if (tid == 0) {  // the basis chunk of (nt, kc) into B stage sb
+            if (!mbar_wait_bounded(b_empty(sb), pb ^ 1u)) {
+              ok = false;
+              atomicOr(err, 1u);
+              break;
+            }
+            unsigned char *bs = sm + Ly.b0 + (size_t)sb * Ly.b_stage;
+            const char *src = reinterpret_cast<const char *>(basis) + (size_t)(nt * S.kchunks + kc) * 2 * b_img;
+            mbar_expect_tx(b_full(sb), SPLIT == 3 ? 2u * b_img : b_img);
+            bulk_g2s(smem_u32(bs), src, b_img, b_full(sb));
+            if (SPLIT == 3) bulk_g2s(smem_u32(bs + Ly.b_img), src + b_img, b_img, b_full(sb));
           }
+          float x[kDftRowCols];
 #pragma unroll
-          for (int q = 0; q < 4; q++) {
+          for (int q = 0; q < kDftRowCols; q++) {
+            x[q] = xn[q];
+            xn[q] = xn2[q];
+          }
+          const int ci = nt * S.kchunks + kc;
+          if (ci + 2 < nchunks)
+            load_row<kDftRowCols>(xn2, sig, s0 + (long long)((kc + 2) % S.kchunks) * kDftKC, cd.length, cd.sig_off,
+                                  a.pad_mode, valid);
+          if (!mbar_wait_bounded(a_empty(sa), pa ^ 1u)) {
+            ok = false;
+            atomicOr(err, 1u);
+            break;
+          }
+          unsigned char *as = sm + Ly.a0 + (size_t)sa * Ly.a_stage;
+#pragma unroll
+          for (int q = 0; q < kDftRowCols / 8; q++) {
             uint4 hi, lo;
             split8(x + 8 * q, hi, lo);
-            const uint32_t off = sw128(row, 32 * half + 8 * q);
-            *reinterpret_cast<uint4 *>(a_hi + off) = hi;
-            if (SPLIT == 3) *reinterpret_cast<uint4 *>(a_lo + off) = lo;
+            const uint32_t off = sw128(row, kDftRowCols * part + 8 * q);
+            *reinterpret_cast<uint4 *>(as + off) = hi;
+            if (SPLIT == 3) *reinterpret_cast<uint4 *>(as + kDftM * 128 + off) = lo;
           }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(a_full(sa));
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (__syncthreads_or(!ok)) {  // an MMA never completed: every thread decides alike
-          failed = true;
-          if (tid == 0) atomicOr(err, 1u);
-          break;
-        }
-        if (tid == 0 && !broken) {
-          if (mbar_wait_bounded(full_bar(st), (full_ph >> st) & 1u)) {
+      }
+    }
+    // bulk copies still in flight write into this CTA's shared memory: wait
+    // for the ones armed last (their phases complete once the bytes land)
+    if (tid == 0)
+      for (uint32_t q = c > (uint32_t)SB ? c - SB : 0; q < c; q++)
+        mbar_wait_bounded(b_full((int)(q % (uint32_t)SB)), (q / (uint32_t)SB) & 1u);
+  } else if (warp == kDftMmaWarp) {
+    // ---------------- MMA issue (one thread)
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(S.tile_cols);
+      uint32_t c = 0, j = 0;  // chunk and accumulator-tile counters
+      bool ok = true;
+      for (int tile = t_begin; tile < t_end && ok; tile++) {
+        for (int nt = 0; nt < S.ntiles && ok; nt++, j++) {
+          const int ab = (int)(j & 1u);
+          if (!mbar_wait_bounded(acc_empty(ab), ((j >> 1) & 1u) ^ 1u)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t acc = tmem + (uint32_t)ab * 256u;
+          for (int kc = 0; kc < S.kchunks; kc++, c++) {
+            const int sa = (int)(c % kDftAStages), sb = (int)(c % (uint32_t)SB);
+            if (!mbar_wait_bounded(a_full(sa), (c / kDftAStages) & 1u) ||
+                !mbar_wait_bounded(b_full(sb), (c / (uint32_t)SB) & 1u)) {
+              ok = false;
+              break;
+            }
             tc_fence_after();
-            const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
-            const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+            const uint32_t ah = smem_u32(sm + Ly.a0 + (size_t)sa * Ly.a_stage), al = ah + kDftM * 128;
+            const uint32_t bh = smem_u32(sm + Ly.b0 + (size_t)sb * Ly.b_stage), bl = bh + (uint32_t)Ly.b_img;
 #pragma unroll
             for (int kk = 0; kk < kDftKC / 16; kk++) {
               const uint64_t dah = desc_sw128(ah + kk * 32), dbh = desc_sw128(bh + kk * 32);
-              umma_bf16(tmem, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
+              umma_bf16(acc, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
               if (SPLIT == 3) {
-                umma_bf16(tmem, dah, desc_sw128(bl + kk * 32), idesc, 1u);
-                umma_bf16(tmem, desc_sw128(al + kk * 32), dbh, idesc, 1u);
+                umma_bf16(acc, dah, desc_sw128(bl + kk * 32), idesc, 1u);
+                umma_bf16(acc, desc_sw128(al + kk * 32), dbh, idesc, 1u);
               }
             }
-            umma_commit(empty_bar(st));
-          } else {  // the basis never arrived: no commit, so the others time out on empty[st]
-            broken = true;
-            atomicOr(err, 1u);
+            umma_commit(a_empty(sa));  // the stages are free once these MMAs complete
+            umma_commit(b_empty(sb));
+          }
+          if (ok) umma_commit(acc_full(ab));
+        }
+      }
+      if (!ok) atomicOr(err, 1u);
+      umma_commit(fin);  // every MMA issued here has completed once this arrives
+      mbar_wait_bounded(fin, 0u);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue: |X|^2 of each N tile and the mel fold, one frame per thread
+    const int row = 32 * (warp & 3) + lane;  // TMEM lane = frame of the tile
+    const uint32_t lane_base = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const int seg_lo = seg_s[0].x, seg_hi = seg_s[nmel].x;
+    const float ref_db = 10.0f * log10f(a.ref);
+    uint32_t j = 0;
+    bool ok = true;
+    int cur_clip = -1;
+    float vmax = -INFINITY;
+    for (int tile = t_begin; tile < t_end && ok; tile++) {
+      const int cl = __ldg(a.tile_clip + tile);
+      if (cl != cur_clip) {
+        float m = vmax;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && cur_clip >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur_clip, enc_f(m));
+        cur_clip = cl;
+        vmax = -INFINITY;
+      }
+      const ClipDesc cd = load_clip(a.clips + cl);
+      const int t = (tile - cd.tile_base) * kDftM + row;
+      const bool valid = t < cd.n_frames;
+      float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
+      int cur = 0;
+      float Rprev = 0.0f, Rcur = 0.0f, Fcur = 0.0f, chk = 0.0f, fmax_ = -INFINITY;
+      auto emit = [&](int m, float v) {
+        if (seg_s[m].y) v = __int_as_float(0x7fc00000);
+        const float val = db10_frame(v, a.amin, ref_db);
+        if (valid) dst[m] = val;
+        fmax_ = fmaxf(fmax_, val);
+      };
+      auto finish_seg = [&]() {
+        if (cur >= 1) emit(cur - 1, Rprev + Fcur);
+        Rprev = Rcur;
+        Rcur = 0.0f;
+        Fcur = 0.0f;
+        cur++;
+      };
+      for (int nt = 0; nt < S.ntiles; nt++, j++) {
+        const int ab = (int)(j & 1u);
+        if (!mbar_wait_bounded(acc_full(ab), (j >> 1) & 1u)) {
+          ok = false;
+          atomicOr(err, 1u);
+          break;
+        }
+        tc_fence_after();
+        const int kb = nt * S.tile_cols / 2;
+        const int nb = min(S.tile_cols / 2, S.nbins - kb);
+        for (int col = 0; col < 2 * nb; col += 16) {
+          float v[16];
+          tmem_ld16(lane_base + (uint32_t)ab * 256u + (uint32_t)col, v);
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int bin = kb + col / 2 + q;
+            if (bin >= kb + nb) break;
+            const float p = fmaf(v[2 * q], v[2 * q], v[2 * q + 1] * v[2 * q + 1]);
+            chk += p;
+            if (bin < seg_lo || bin >= seg_hi) continue;
+            while (cur < nmel && bin >= seg_s[cur + 1].x) finish_seg();
+            const float2 w = w2_s[bin];
+            Rcur = fmaf(w.x, p, Rcur);
+            Fcur = fmaf(w.y, p, Fcur);
           }
         }
-        full_ph ^= bit;
-        pend |= bit;
-        chunk++;
+        tc_fence_before();
+        mbar_arrive(acc_empty(ab));  // the accumulator may take the next N tile after next
       }
-      if (failed) break;
-      // ---- drain: the tile's accumulator is complete
-      bool ok = true;
-      for (int st = 0; st < kDftStages; st++)
-        if (pend & (1u << st)) {
-          ok = mbar_wait_bounded(empty_bar(st), (empty_ph >> st) & 1u) && ok;
-          empty_ph ^= 1u << st;
-          pend &= ~(1u << st);
-        }
-      if (__syncthreads_or(!ok)) {
-        failed = true;
-        if (tid == 0) atomicOr(err, 1u);
-        break;
-      }
-      tc_fence_after();
-      // ---- |X|^2 of this tile's bins into P[bin][frame]; the two warps of a
-      // lane quarter take alternate 16-column pieces
-      const int kb = nt * S.tile_cols / 2;
-      const int nb = min(S.tile_cols / 2, S.nbins - kb);
-      for (int col = 16 * half; col < 2 * nb; col += 32) {
-        float v[16];
-        tmem_ld16(lane_base + (uint32_t)col, v);
-#pragma unroll
-        for (int b = 0; b < 8; b++) {
-          const int bin = col / 2 + b;
-          if (bin < nb) P[bin * kDftM + row] = fmaf(v[2 * b], v[2 * b], v[2 * b + 1] * v[2 * b + 1]);
-        }
-      }
-      __syncthreads();
-      if (half == 0) {
-        for (int bin = 0; bin < nb; bin++) chk += P[bin * kDftM + row];
-        // ---- fold this tile's bins into the mel bands (uniform control flow)
-        for (int bin = max(kb, seg_lo); bin < min(kb + nb, seg_hi); bin++) {
-          while (cur < nmel && bin >= seg_s[cur + 1].x) finish_seg();
-          const float2 w = w2_s[bin];
-          const float p = P[(bin - kb) * kDftM + row];
-          Rcur = fmaf(w.x, p, Rcur);
-          Fcur = fmaf(w.y, p, Fcur);
-        }
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // P reads before later bulk copies
-      tc_fence_before();
-      __syncthreads();  // P (aliasing the stages) and the accumulator are free again
-    }
-    if (failed) break;
-    if (half == 0) {
+      if (!ok) break;
       while (cur < nmel) finish_seg();
       if (nmel > 0) emit(nmel - 1, Rprev);
       if (!isfinite(chk)) {  // a non-finite bin: every band of the frame is NaN -> amin
-        const float val = db10_frame(a.amin, a.amin, 10.0f * log10f(a.ref));
+        const float val = db10_frame(a.amin, a.amin, ref_db);
         if (valid)
           for (int m = 0; m < nmel; m++) dst[m] = val;
         fmax_ = val;
       }
       if (valid) vmax = fmaxf(vmax, fmax_);
     }
-  }
-  if (!failed) {
-    float m = vmax;
+    if (ok) {
+      float m = vmax;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((tid & 31) == 0 && cur_clip >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur_clip, enc_f(m));
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (lane == 0 && cur_clip >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur_clip, enc_f(m));
+    }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0)
+  if (warp == kDftMmaWarp)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDftTmemCols) : "memory");
 }
 
@@ -511,14 +564,14 @@ cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, con
   if (launched) *launched = 0;
   if (a.total_tiles <= 0) return cudaSuccess;
   if (!a.mel_seg_ok) return cudaErrorInvalidValue;  // the epilogue needs the per-bin split
-  const size_t smem = std::max(dft_smem_layout(s, a.n_mels).total, kDftMinSmem);
+  if (s.tile_cols > 256) return cudaErrorInvalidValue;
+  const size_t smem = dft_smem_layout(s, a.n_mels).total;
   const void *kern = form == DFT_GEMM_BF16X3 ? reinterpret_cast<const void *>(dft_gemm_kernel<3>)
                                               : reinterpret_cast<const void *>(dft_gemm_kernel<1>);
   int per_sm = 1, sms = 148;
   cudaError_t e = persistent_geometry(kern, kDftThreads, smem, &per_sm, &sms);
   if (e != cudaSuccess) return e;
-  per_sm = std::min(per_sm, 512 / kDftTmemCols);
-  long long grid = (long long)sms * per_sm;
+  long long grid = sms;  // one CTA per SM: it holds all 512 TMEM columns
   if (grid > a.total_tiles) grid = a.total_tiles;
   if (form == DFT_GEMM_BF16X3)
     dft_gemm_kernel<3><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);

@@ -52,13 +52,33 @@ int run_batch(const Group &g_in, const float *const *signals, const int64_t *len
   cudaStream_t s = ws->stream;
   cudaError_t e = cudaStreamSynchronize(s);  // staging buffer is free again
   if (e != cudaSuccess) return cuda_status(e);
-  // Stage signals + descriptors in pinned memory, then one async copy each.
+  // Signals: a large clip goes straight from the caller's (pageable) buffer,
+  // where the driver overlaps its own staging with the transfer (measured
+  // ~150 us for 2.6 MB, against ~210 us for a copy into pinned staging then
+  // an upload); small clips are gathered in pinned memory and uploaded in
+  // one copy.  Descriptors always come from pinned memory.
+  // The staged region (which spans the large clips' slots too) is uploaded
+  // first, so that the direct copies, later in stream order, land on top.
   char *h = ws->host;
-  for (int i = 0; i < n; i++)
-    memcpy(h + sizeof(float) * (size_t)L.clips[i].sig_off, signals[i], sizeof(float) * (size_t)lengths[i]);
+  constexpr size_t kDirect = size_t(1) << 20;
+  bool staged = false;
+  for (int i = 0; i < n; i++) {
+    const size_t bytes = sizeof(float) * (size_t)lengths[i];
+    if (bytes < kDirect) {
+      memcpy(h + sizeof(float) * (size_t)L.clips[i].sig_off, signals[i], bytes);
+      staged = true;
+    }
+  }
   pack_descriptors(L, h + sig_bytes);
-  if ((e = cudaMemcpyAsync(b.signal, h, sig_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+  if (staged && (e = cudaMemcpyAsync(b.signal, h, sig_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_status(e);
+  for (int i = 0; i < n; i++) {
+    const size_t bytes = sizeof(float) * (size_t)lengths[i];
+    if (bytes >= kDirect &&
+        (e = cudaMemcpyAsync(b.signal + L.clips[i].sig_off, signals[i], bytes, cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess)
+      return cuda_status(e);
+  }
   if ((e = cudaMemcpyAsync(b.clips, h + sig_bytes, desc_bytes, cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_status(e);
   if ((e = enqueue_batch(g, L, t, b, s, nullptr, nullptr)) != cudaSuccess) return cuda_status(e);

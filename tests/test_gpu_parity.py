@@ -468,3 +468,17 @@ def test_warp_kernel_filterbank_shapes_vs_oracle(n_fft, n_mels, fmin, fmax):
     exp = O.mfcc(y, SR, n_mfcc, n_fft, n_fft // 4, n_fft, n_mels, fmin, fmax)
     assert got.shape == exp.shape
     assert O.mfcc_rel_error(got, exp) < MFCC_TOL, O.mfcc_rel_error(got, exp)
+
+
+def test_batch_mixing_short_and_long_clips_matches_single_calls():
+    """Clips of 1 MB and more are uploaded from the caller's buffer, shorter
+    ones through pinned staging whose upload spans the whole signal region;
+    in a batch that mixes both, every clip's result equals its single-clip
+    result bitwise."""
+    lens = [1000, 300000, 5000, 400000, 262144, 262143]
+    clips = [synth.music_clip(L, SR, seed=70 + i) for i, L in enumerate(lens)]
+    outs = M.mfcc_batch(clips, sr=SR, n_fft=2048, hop_length=512)
+    for c, o in zip(clips, outs):
+        np.testing.assert_array_equal(o, M.mfcc(c, sr=SR, n_fft=2048, hop_length=512))
+    exp = O.mfcc(clips[1], SR, 20, 2048, 512, 2048, 128)
+    assert O.mfcc_rel_error(outs[1], exp) < MFCC_TOL

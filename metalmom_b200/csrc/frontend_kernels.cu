@@ -195,8 +195,7 @@ frontend_kernel(FrontArgs a) {
   sp += 16 * (size_t)nmel;
   float *melw_s = reinterpret_cast<float *>(sp);
   if (mel_in_smem) sp += align16(4 * (size_t)a.mel_nnz);
-  float *red_s = reinterpret_cast<float *>(sp);
-  sp += 128;
+  sp += 128;  // (a reserved 128-byte slot of the layout)
   int *bad_s = reinterpret_cast<int *>(sp);
   sp += align16(F * 4);
   cpx *tws_s = reinterpret_cast<cpx *>(sp);
@@ -1492,7 +1491,7 @@ __global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
 // Coefficient groups: kg 0, 1 take even k = 2 (KQ kg + q), kg 2, 3 odd
 // k = 2 (KQ (kg - 2) + q) + 1, so KQ = ceil(ceil(n_mfcc / 2) / 2).
 template <int KQ>
-__global__ void __launch_bounds__(256, 2) dct_fold_kernel(DctArgs a) {
+__global__ void __launch_bounds__(256, 3) dct_fold_kernel(DctArgs a) {
   constexpr int NM = 128, H = NM / 2, H4 = H / 4;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) float dsm[];

@@ -1,0 +1,80 @@
+"""Seeded random front-end configurations against the FP64 oracle.
+
+Each case draws a sample rate, n_fft (16..4096), hop, window length,
+band count, fmin / fmax, MFCC count, clip length and padding, and checks
+mm_mfcc (MFCC within 1e-4 of max |c|) and mm_mel_spectrogram through the C
+ABI, and the batched entry point with the clip in a mixed batch (bitwise
+equal to the single call).
+
+Mel-dB tolerance: 1e-3 dB for values within 60 dB of the clip's maximum,
+1e-2 dB below that.  The float32 FFT's rounding is absolute (a fraction of
+the frame's largest bins), so its dB error grows with the distance below the
+maximum: measured on these draws, <= 4.3e-5 dB within 40 dB, <= 4.1e-4 dB
+within 60 dB, up to 3e-3 dB for the few values 60-80 dB down that the top_db
+floor keeps (small n_fft, high dynamic range); the reference's float32 path
+rounds the same way.
+
+The draw covers the kernel choices the library makes on its own: the warp
+kernel with lane tables or packed rows, the CTA-tile kernels of every size and
+the tiny direct-DFT kernel.
+"""
+
+import numpy as np
+import pytest
+
+import metalmom_b200 as M
+from metalmom_b200 import synth
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MFCC_TOL = 1e-4
+DB_TOL = 1e-3
+
+
+def _draw(seed):
+    rng = np.random.default_rng(seed)
+    sr = int(rng.choice([8000, 16000, 22050, 44100]))
+    n_fft = int(2 ** rng.integers(4, 13))
+    hop = int(max(1, n_fft // int(rng.choice([1, 2, 3, 4, 8]))))
+    win = int(rng.integers(max(1, n_fft // 4), n_fft + 1)) if rng.random() < 0.4 else n_fft
+    n_mels = int(rng.integers(1, min(160, 8 + n_fft // 8)))
+    fmin = float(rng.choice([0.0, 20.0, 100.0, 300.0]))
+    fmax = None if rng.random() < 0.5 else float(rng.uniform(fmin + 500.0, sr / 2.0))
+    n_mfcc = int(rng.integers(1, 40))
+    L = int(rng.integers(1, 4 * sr))
+    pad = "reflect" if (rng.random() < 0.25 and L > n_fft // 2) else "constant"
+    return dict(sr=sr, n_fft=n_fft, hop=hop, win=win, n_mels=n_mels, fmin=fmin, fmax=fmax, n_mfcc=n_mfcc, L=L,
+                pad=pad)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_config_vs_oracle(seed):
+    c = _draw(seed)
+    y = synth.music_clip(c["L"], c["sr"], seed=seed)
+    pm = O.PAD_REFLECT if c["pad"] == "reflect" else O.PAD_CONSTANT
+    kw = dict(sr=c["sr"], n_fft=c["n_fft"], hop_length=c["hop"], win_length=c["win"], n_mels=c["n_mels"],
+              fmin=c["fmin"], fmax=c["fmax"])
+    exp = O.mfcc(y, c["sr"], c["n_mfcc"], c["n_fft"], c["hop"], c["win"], c["n_mels"], c["fmin"], c["fmax"], True,
+                 pad_mode=pm)
+    if c["pad"] == "constant":  # the reference's per-clip entry points pad with zeros only
+        got = M.mfcc(y, n_mfcc=c["n_mfcc"], **kw)
+        assert got.shape == exp.shape, c
+        if exp.size:
+            assert O.mfcc_rel_error(got, exp) < MFCC_TOL, (c, O.mfcc_rel_error(got, exp))
+        mel = M.melspectrogram(y, **kw)
+        got_db = O.power_to_db(np.asarray(mel, np.float64), 1.0, 1e-10, 80.0)
+        exp_db = O.mel_db(y, c["sr"], c["n_fft"], c["hop"], c["win"], True, c["n_mels"], c["fmin"], c["fmax"])
+        if exp_db.size:
+            near = exp_db >= exp_db.max() - 60.0
+            err = np.abs(got_db - exp_db)
+            assert err[near].max() < DB_TOL, (c, err[near].max())
+            assert err.max() < 10 * DB_TOL, (c, err.max())
+    # batched, with the padding mode of the draw, next to a clip of another length
+    other = synth.music_clip(c["L"] // 3 + 7, c["sr"], seed=seed + 1000)
+    bkw = dict(kw, n_mfcc=c["n_mfcc"], pad_mode=c["pad"])
+    outs = M.mfcc_batch([other, y], **bkw)
+    assert outs[1].shape == exp.shape, c
+    if exp.size:
+        assert O.mfcc_rel_error(outs[1], exp) < MFCC_TOL, (c, O.mfcc_rel_error(outs[1], exp))
+    np.testing.assert_array_equal(outs[1], M.mfcc_batch([y], **bkw)[0])

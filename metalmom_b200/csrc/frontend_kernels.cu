@@ -381,19 +381,25 @@ frontend_kernel(FrontArgs a) {
       pmid = z.x * z.x + z.y * z.y;
     }
     frame_sync<TPF>(f);
+    // the log-mel epilogue's filterbank walk reads the spectrum padded (bin k
+    // at k + min(k / 32, TW - 1), TW = TPF / 2 walking threads of 32 bins), so
+    // that its 32 bins per thread are conflict-free rows of 33
+    constexpr int TW = TPF / 2;
+    const bool walk = MODE == MODE_MELDB && a.mel_lane_ok;
+    auto pk = [&](int k) { return walk ? k + min(k >> 5, TW - 1) : k; };
     float chk = 0.0f;  // sum of this thread's |X|^power: non-finite iff one term is
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int k = j + i * TPF;
       const float x = apply_power<PW>(pa[i], a.power);
       const float y = apply_power<PW>(pb[i], a.power);
-      P[k] = x;
-      P[M - k] = y;
+      P[pk(k)] = x;
+      P[pk(M - k)] = y;
       chk += x + y;
     }
     if (j == 0) {
       const float x = apply_power<PW>(pmid, a.power);
-      P[M / 2] = x;
+      P[pk(M / 2)] = x;
       chk += x;
     }
     const bool bad = frame_sync_or<TPF>(f, !isfinite(chk));
@@ -403,11 +409,66 @@ frontend_kernel(FrontArgs a) {
       const bool valid = t < cd.n_frames;
       float vmax = -INFINITY;
       float *dst = a.out + (cd.frame_off + t) * (long long)a.n_mels;
-      for (int m = j; m < a.n_mels; m += TPF) {
-        const float acc = mel_dot(mel_s[m], melw, P, bad);
-        const float v = db10_frame(acc, a.amin, 10.0f * log10f(a.ref));
-        if (valid) dst[m] = v;
-        vmax = fmaxf(vmax, v);
+      const float ref_db = 10.0f * log10f(a.ref);
+      if (walk) {
+        // the warp kernel's filterbank walk (tables at build_mel_lane_kernel):
+        // thread j < TW sums its 32 bins into part slots, segment heads take
+        // the parts of the threads they run into, a band is two slot reads
+        float2 *parts = reinterpret_cast<float2 *>(P + 33 * TW);
+        int hslot = 0, chain = 0;
+        if (j < TW) {
+          const int2 li = __ldg(a.mel_lane + j);
+          const unsigned fl = (unsigned)li.x;
+          int slot = li.y & 1023;
+          const float *pl = P + 33 * j;
+          float R = 0.0f, Fs = 0.0f;
+#pragma unroll
+          for (int b = 0; b < 32; b++) {
+            const float p = pl[b];
+            const float2 w = __ldg(a.mel_lw + b * TW + j);
+            R = fmaf(w.x, p, R);
+            Fs = fmaf(w.y, p, Fs);
+            if (fl & (1u << b)) {
+              parts[slot++] = make_float2(R, Fs);
+              R = 0.0f;
+              Fs = 0.0f;
+            }
+          }
+          if (j == TW - 1) {
+            const float p = pl[32];
+            const float2 w = __ldg(a.mel_lw + 32 * TW + j);
+            parts[slot] = make_float2(fmaf(w.x, p, R), fmaf(w.y, p, Fs));
+          }
+          if (j == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);  // the empty segments' slot
+          hslot = j == TW - 1 ? slot : slot - 1;
+          chain = (li.y >> 10) & 63;
+        }
+        frame_sync<TPF>(f);
+        if (chain) {
+          float2 hv = parts[hslot];
+          for (int q = 1; q <= chain; q++) {
+            const float2 pv = parts[hslot + q];
+            hv.x += pv.x;
+            hv.y += pv.y;
+          }
+          parts[hslot] = hv;
+        }
+        frame_sync<TPF>(f);
+        for (int m = j; m < a.n_mels; m += TPF) {
+          const int bw = __ldg(a.mel_band + m);
+          float acc = parts[bw & 4095].x + parts[(bw >> 12) & 4095].y;
+          if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
+          const float v = db10_frame(acc, a.amin, ref_db);
+          if (valid) dst[m] = v;
+          vmax = fmaxf(vmax, v);
+        }
+      } else {
+        for (int m = j; m < a.n_mels; m += TPF) {
+          const float acc = mel_dot(mel_s[m], melw, P, bad);
+          const float v = db10_frame(acc, a.amin, ref_db);
+          if (valid) dst[m] = v;
+          vmax = fmaxf(vmax, v);
+        }
       }
       if (!valid) vmax = -INFINITY;
       constexpr int W = TPF < 32 ? TPF : 32;
@@ -909,10 +970,10 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
                                       const int2 *seg, int n_mels, int tpf, int max_slots, int *ok) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   ok[2] = 0;
-  if (!ok[1] || tpf > 32) return;
+  if (!ok[1] || tpf > 64) return;
   for (int m = 0; m < n_mels; m++) band[m] = 0;  // first(s) | count(s) << 12 during the walk
   int slot = 0, sid = -1;
-  int last_slot[32], last_sid[32];
+  int last_slot[64], last_sid[64];
   // segment of bin k: the band of the last bin at or below k that feeds one
   // (bins with no band carry on the run before them, with zero weights)
   auto next_sid = [&](int k, int cur) { return bin_seg[k] >= 0 ? bin_seg[k] : cur; };

@@ -149,13 +149,19 @@ int frame_variants(int log2n, int mode, int power_is_2);
 // Launch variant 3: the warp-per-frame kernel (MODE_MELDB, n_fft 256..2048).
 constexpr int kWarpVariant = 3;
 int warp_frames_per_tile(int log2n);  // 0 when the size has no warp kernel
-// Lanes per frame of the warp kernel (n_fft / 64) for n_fft 256..2048, else 0.
+// Walking lanes of the filterbank walk (n_fft / 64, 32 bins each) for n_fft
+// 256..4096, else 0: the warp kernel's lanes (up to 2048), or the first
+// n_fft / 64 threads of a frame in the CTA-tile kernel.
 inline int mel_lane_tpf(int n_fft) {
-  return (n_fft >= 256 && n_fft <= 2048 && (n_fft & (n_fft - 1)) == 0) ? n_fft / 64 : 0;
+  return (n_fft >= 256 && n_fft <= 4096 && (n_fft & (n_fft - 1)) == 0) ? n_fft / 64 : 0;
 }
-// Filterbank part slots that fit in a frame buffer (66 tpf floats) behind the
-// padded spectrum (33 tpf floats, starting tpf g floats in for frame group g).
-inline int mel_lane_max_slots(int tpf) { return tpf > 0 ? (33 * tpf - tpf * (32 / tpf - 1)) / 2 : 0; }
+// Filterbank part slots that fit behind the padded spectrum (33 tpf floats):
+// in a warp-kernel frame buffer (66 tpf floats, frame group g starting tpf g
+// floats in) for tpf <= 32; 1024 (the slot field's range) for tpf = 64, whose
+// CTA-tile frame buffer holds more than 33 tpf + 2048 floats.
+inline int mel_lane_max_slots(int tpf) {
+  return tpf <= 0 ? 0 : (tpf <= 32 ? (33 * tpf - tpf * (32 / tpf - 1)) / 2 : 1024);
+}
 cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,
                                  int *launched);
 // Stockham twiddle table length (entries) for log2(n_fft) >= 5.

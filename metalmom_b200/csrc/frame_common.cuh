@@ -82,6 +82,40 @@ __device__ __forceinline__ cpx ldc(const float2 *p) {
 
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
+// Barrier over the TPF threads of frame group f, returning the OR of `pred`
+// over the group.  Groups of >= 32 threads use named barrier f+1; smaller
+// groups live inside one warp.
+template <int TPF>
+__device__ __forceinline__ bool frame_sync_or(int f, bool pred) {
+  if constexpr (TPF >= 32) {
+    unsigned r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.or.pred p, %2, %3, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(r)
+        : "r"((unsigned)pred), "r"(f + 1), "r"(TPF)
+        : "memory");
+    return r != 0;
+  } else {
+    __syncwarp();
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned mask = ((TPF == 32) ? 0xffffffffu : ((1u << TPF) - 1u)) << (lane & ~(unsigned)(TPF - 1));
+    const unsigned b = __ballot_sync(0xffffffffu, pred);
+    return (b & mask) != 0;
+  }
+}
+
+template <int TPF>
+__device__ __forceinline__ void frame_sync(int f) {
+  if constexpr (TPF >= 32) {
+    asm volatile("bar.sync %0, %1;" ::"r"(f + 1), "r"(TPF) : "memory");
+  } else {
+    __syncwarp();
+  }
+}
+
 // Packed mel weights are staged in shared memory up to this size.
 constexpr int kMelSmemMax = 12288;  // floats
 // Shared-memory bytes for the mel tables: per-mel info + packed weights (when they fit).

@@ -39,40 +39,6 @@ float decode_max(unsigned u) {
   return f;
 }
 
-// Barrier over the TPF threads of frame group f, returning the OR of `pred`
-// over the group.  Groups of >= 32 threads use named barrier f+1; smaller
-// groups live inside one warp.
-template <int TPF>
-__device__ __forceinline__ bool frame_sync_or(int f, bool pred) {
-  if constexpr (TPF >= 32) {
-    unsigned r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 q, %1, 0;\n\t"
-        "bar.red.or.pred p, %2, %3, q;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(r)
-        : "r"((unsigned)pred), "r"(f + 1), "r"(TPF)
-        : "memory");
-    return r != 0;
-  } else {
-    __syncwarp();
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned mask = ((TPF == 32) ? 0xffffffffu : ((1u << TPF) - 1u)) << (lane & ~(unsigned)(TPF - 1));
-    const unsigned b = __ballot_sync(0xffffffffu, pred);
-    return (b & mask) != 0;
-  }
-}
-
-template <int TPF>
-__device__ __forceinline__ void frame_sync(int f) {
-  if constexpr (TPF >= 32) {
-    asm volatile("bar.sync %0, %1;" ::"r"(f + 1), "r"(TPF) : "memory");
-  } else {
-    __syncwarp();
-  }
-}
-
 // ---------------------------------------------------------------------------
 // FFT shape for a real frame of N = 2^LOG2N samples (complex length M = N/2):
 // radix-16 stages followed by one radix-RLAST stage when log2(M) % 4 != 0.
@@ -971,7 +937,9 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   ok[2] = 0;
   if (!ok[1] || tpf > 64) return;
-  for (int m = 0; m < n_mels; m++) band[m] = 0;  // first(s) | count(s) << 12 during the walk
+  // first(s) | count(s) << 12 during the walk; a segment has one part per
+  // lane it touches, so count <= 64 (7 bits) and its chain k = count - 1 <= 63
+  for (int m = 0; m < n_mels; m++) band[m] = 0;
   int slot = 0, sid = -1;
   int last_slot[64], last_sid[64];
   // segment of bin k: the band of the last bin at or below k that feeds one
@@ -992,7 +960,7 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
       if (sid >= 0) {
         if (slot >= 1023 || sid >= n_mels) return;
         int w = band[sid];
-        if (((w >> 12) & 63) == 0) w = slot;  // first part of segment sid
+        if (((w >> 12) & 127) == 0) w = slot;  // first part of segment sid
         w += 1 << 12;
         band[sid] = w;
       }
@@ -1008,12 +976,12 @@ __global__ void build_mel_lane_kernel(float2 *lw, int2 *lane, int *band, const f
   for (int l = 0; l < tpf; l++) {
     const int s = last_sid[l];
     int k = 0;
-    if (s >= 0 && last_slot[l] == (band[s] & 4095)) k = ((band[s] >> 12) & 63) - 1;  // lane l holds the head
+    if (s >= 0 && last_slot[l] == (band[s] & 4095)) k = ((band[s] >> 12) & 127) - 1;  // lane l holds the head
     lane[l].y |= (k << 10) | (zero << 16);
   }
   for (int m = 0; m < n_mels; m++) {  // band[m + 1] is still in the walk's form when band[m] is rewritten
-    const int hr = ((band[m] >> 12) & 63) ? (band[m] & 4095) : zero;
-    const int hf = (m + 1 < n_mels && ((band[m + 1] >> 12) & 63)) ? (band[m + 1] & 4095) : zero;
+    const int hr = ((band[m] >> 12) & 127) ? (band[m] & 4095) : zero;
+    const int hf = (m + 1 < n_mels && ((band[m + 1] >> 12) & 127)) ? (band[m + 1] & 4095) : zero;
     band[m] = hr | (hf << 12) | ((seg[m].y ? 1 : 0) << 24);
   }
   ok[2] = 1;

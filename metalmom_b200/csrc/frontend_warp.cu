@@ -1,5 +1,5 @@
 // Warp-per-frame front-end kernel (launch variant 3, n_fft 256..2048, MFCC
-// path): framing + periodic Hann + real FFT + |X|^2 + Slaney mel + log10 per
+// path; n_fft 4096 on a warp pair, frame_warp2_kernel below): framing + periodic Hann + real FFT + |X|^2 + Slaney mel + log10 per
 // frame, with a running per-clip maximum for top_db.
 //
 // The reference computes the same per frame on the CPU, one frame after the
@@ -196,6 +196,7 @@ int warp_frames_per_tile(int log2n) {
     case 9: return WShape<9>::F;
     case 10: return WShape<10>::F;
     case 11: return WShape<11>::F;
+    case 12: return 8;  // frame_warp2_kernel: one frame per warp pair, 16 warps
     default: return 0;
   }
 }
@@ -563,6 +564,325 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
 }
 
+// ---------------------------------------------------------------------------
+// n_fft 4096: one frame per pair of warps (64 threads), same per-frame work.
+//
+//   n = j + 64 r (j < 64: thread of the pair, r < 32), k = k1 + 32 k2 (k2 < 64)
+//   stage 1: 32-point DFT over r in registers, twiddle W_M^(j k1), row j of
+//            the frame buffer (stride 33)
+//   stage 2: the 64-point DFT over j of column k1 as 2 x 32: thread (k1, j0)
+//            takes rows j0 + 2 j1 (j1 < 32) through a 32-point DFT -> A_j0[q];
+//            the two threads of a column (lanes 2i, 2i+1) swap half of their
+//            outputs by shuffle, and thread j0 forms
+//            Z[k1 + 32 q] = A_0[q] + W_64^q A_1[q] and
+//            Z[k1 + 32 (q + 32)] = A_0[q] - W_64^q A_1[q] for q = 2 i + j0.
+//   Even columns live in the pair's first warp, odd ones in its second
+//   (lane = 2 (k1 >> 1) + j0), so the real-split partner (32 - k1, 1 - j0)
+//   of a thread sits in its warp; the two swap their upper 16 registers as
+//   in the single-warp kernel.  Column 0 pairs inside each thread.
+// Every shared-memory pattern (row stores, column loads, twiddles, spectrum
+// stores, the walk) is conflict-free for this lane assignment.
+// ---------------------------------------------------------------------------
+struct W2Shape {
+  static constexpr int N = 4096;
+  static constexpr int M = N / 2;
+  static constexpr int TPF = 64;            // threads per frame
+  static constexpr int FSTRIDE = TPF * 33;  // complex slots per frame buffer
+  static constexpr int NW = 16;             // warps per CTA (one CTA per SM)
+  static constexpr int THREADS = 32 * NW;
+  static constexpr int F = NW / 2;          // frames per CTA tile
+  static constexpr int RS = 33 * 32;        // real-split twiddles W_N^(c + 32 s) at 33 s + c
+  static constexpr int MEL_SMEM_MAX = 8192; // packed weights staged up to this many floats
+};
+
+__host__ __device__ constexpr size_t warp2_fixed_smem() {
+  using S = W2Shape;
+  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + align16(size_t(S::RS) * 8) +
+         size_t(S::F) * S::FSTRIDE * 8;
+}
+
+__global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontArgs a) {
+  using S = W2Shape;
+  constexpr int N = S::N, M = S::M, TPF = S::TPF, F = S::F;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int nmel = a.n_mels;
+  const float ref_db = 10.0f * log10f(a.ref);
+  const bool lanes = a.mel_lane_ok != 0;
+  const bool mel_in_smem = a.mel_nnz <= S::MEL_SMEM_MAX;
+  unsigned char *sp = smem;
+  cpx *tw2 = reinterpret_cast<cpx *>(sp);  // W_M^(j k1), [k1-1][j]
+  sp += align16(size_t(31) * TPF * 8);
+  float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
+  sp += align16(size_t(N) * 4);
+  cpx *rs_tw = reinterpret_cast<cpx *>(sp);  // W_N^(c + 32 s) at 33 s + c
+  sp += align16(size_t(S::RS) * 8);
+  cpx *bufs = reinterpret_cast<cpx *>(sp);
+  sp += size_t(F) * S::FSTRIDE * 8;
+  // lanes: band words, lane words, lane-minor weights; else packed weights
+  // (the packed rows' descriptors are read from global memory)
+  int *band_s = reinterpret_cast<int *>(sp);
+  int2 *lane_s = reinterpret_cast<int2 *>(sp + align16(4 * (size_t)nmel));
+  float2 *lw_s = reinterpret_cast<float2 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);
+  float *melw_s = reinterpret_cast<float *>(sp);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int fp = warp >> 1;              // frame of this warp pair within the tile
+  const int half = warp & 1;             // 0: even columns, 1: odd columns
+  const int j = half * 32 + lane;        // stage-1 row, walk lane
+  const int j0 = lane & 1;               // stage-2 half of the column
+  const int col = 2 * (lane >> 1) + half;  // stage-2 column k1
+  const bool c0 = col == 0;
+  const int partner = 2 * (half ? 15 - (lane >> 1) : (16 - (lane >> 1)) & 15) + (1 - j0);
+  const float2 *twq = a.tw_split;  // W_N^t, t < N/4
+
+  for (int i = tid; i < 31 * TPF; i += S::THREADS) {
+    const int k1 = i / TPF + 1, jj = i - (k1 - 1) * TPF;
+    tw2[i] = root_q(twq, 2 * jj * k1, N);
+  }
+  for (int i = tid; i < N / 4; i += S::THREADS)
+    reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+  for (int i = tid; i < S::RS; i += S::THREADS) {
+    const int s = i / 33, cc = i - 33 * s;
+    rs_tw[i] = cc < 32 ? root_q(twq, cc + 32 * s, N) : cpx{0.0f, 0.0f};
+  }
+  if (lanes) {
+    for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
+    for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
+    for (int i = tid; i < 33 * TPF; i += S::THREADS) lw_s[i] = __ldg(a.mel_lw + i);
+  } else if (mel_in_smem) {
+    for (int i = tid; i < a.mel_nnz; i += S::THREADS) melw_s[i] = __ldg(a.mel_pw + i);
+  }
+  const float *melw = mel_in_smem ? melw_s : a.mel_pw;
+  __syncthreads();
+
+  // W_64^j0: the odd half's extra rotation in the column combine
+  const cpx w1 = j0 ? cpx{(float)ce_trig(1, 64, 0), -(float)ce_trig(1, 64, 1)} : cpx{1.0f, 0.0f};
+
+  cpx *fb = bufs + fp * S::FSTRIDE;
+  // power spectrum, padded: bin k at k + min(k / 32, 63), so that walk lane
+  // j reads its bins [32 j, 32 j + 32) at 33 j + b and the Nyquist bin at 2111
+  float *P = reinterpret_cast<float *>(fb);
+
+  const int total = a.total_tiles;
+  const int t_begin = (int)((long long)blockIdx.x * total / gridDim.x);
+  const int t_end = (int)((long long)(blockIdx.x + 1) * total / gridDim.x);
+  int cur = -1;
+  float vmax = -INFINITY;
+
+  for (int tile = t_begin; tile < t_end; tile++) {
+    const int cl = __ldg(a.tile_clip + tile);
+    if (cl != cur) {  // CTA-uniform: every frame of a tile belongs to one clip
+      float m = vmax;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+      if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+      cur = cl;
+      vmax = -INFINITY;
+    }
+    const ClipDesc cd = load_clip(a.clips + cl);
+    const int t = (tile - cd.tile_base) * F + fp;
+    if (t >= cd.n_frames) continue;  // uniform over the warp pair
+    const long long s0 = (long long)t * a.hop - a.pad;
+    const float *sig = a.signal + cd.sig_off;
+
+    // ---- gather: v[r] = (x[2n], x[2n+1]) for n = j + 64 r
+    cpx v[32];
+    if (s0 >= 0 && s0 + N <= cd.length) {
+      const float *base = sig + s0 + 2 * j;
+      if (((cd.sig_off + s0) & 1) == 0) {
+#pragma unroll
+        for (int r = 0; r < 32; r++) {
+          const float2 x = __ldg(reinterpret_cast<const float2 *>(base + 2 * TPF * r));
+          v[r] = {x.x, x.y};
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 32; r++) v[r] = {__ldg(base + 2 * TPF * r), __ldg(base + 2 * TPF * r + 1)};
+      }
+    } else {
+      cpx tmp[32];
+      gather_edge(tmp, sig, s0 + 2 * j, cd.length, a.pad_mode, 2 * TPF);
+#pragma unroll
+      for (int r = 0; r < 32; r++) v[r] = tmp[r];
+    }
+    // ---- window
+    {
+      const float2 *wb = reinterpret_cast<const float2 *>(win_s) + j;
+#pragma unroll
+      for (int r = 0; r < 32; r++) {
+        const float2 w = wb[TPF * r];
+        v[r].x *= w.x;
+        v[r].y *= w.y;
+      }
+    }
+
+    // ---- stage 1: 32-point DFT over registers, twiddle, row j of the buffer
+    frame_sync<TPF>(fp);  // the previous frame's band reads of the buffer are done
+    {
+      cpx e[16], o[16];
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        e[m] = v[2 * m];
+        o[m] = v[2 * m + 1];
+      }
+      dft16(e);
+      dft16(o);
+      cpx *row = fb + j * 33;
+      static_for<0, 16>([&](auto ki) {
+        constexpr int k = decltype(ki)::value;
+        const cpx tt = tw_const<k, 32>(o[k]);
+        cpx lo = cadd(e[k], tt), hi = csub(e[k], tt);
+        if constexpr (k > 0) lo = cmul(lo, tw2[(k - 1) * TPF + j]);
+        hi = cmul(hi, tw2[(k + 15) * TPF + j]);
+        row[k] = lo;
+        row[k + 16] = hi;
+      });
+    }
+    frame_sync<TPF>(fp);
+    // ---- stage 2a: 32-point DFT of rows j0 + 2 j1 of column col -> A_j0[q]
+#pragma unroll
+    for (int j1 = 0; j1 < 32; j1++) v[j1] = fb[(j0 + 2 * j1) * 33 + col];
+    dft32(v);
+    // ---- stage 2b: combine the column's two halves; z[i] = Z[col + 32 (2i + j0)],
+    // z[16 + i] = Z[col + 32 (2i + j0 + 32)]
+    cpx z[32];
+    static_for<0, 16>([&](auto ii) {
+      constexpr int i = decltype(ii)::value;
+      const cpx snd = j0 ? v[2 * i] : v[2 * i + 1];
+      cpx rcv;
+      rcv.x = __shfl_xor_sync(FULL, snd.x, 1);
+      rcv.y = __shfl_xor_sync(FULL, snd.y, 1);
+      const cpx ev = j0 ? rcv : v[2 * i];
+      cpx od = tw_const<2 * i, 64>(j0 ? v[2 * i + 1] : rcv);
+      od = cmul(od, w1);
+      z[i] = cadd(ev, od);
+      z[16 + i] = csub(ev, od);
+    });
+    // ---- real split: pair i is (Z[k], Z[M - k]), k = col + 32 (2i + j0); the
+    // partner's z[31 - i] holds Z[M - k] (column 0: this thread's own z)
+    cpx rcv[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      rcv[m].x = __shfl_sync(FULL, z[16 + m].x, partner);
+      rcv[m].y = __shfl_sync(FULL, z[16 + m].y, partner);
+    }
+    frame_sync<TPF>(fp);  // every column is read: the buffer becomes P
+    {
+      float *Pa = P + col + 33 * j0;                         // bin col + 32 s at col + 33 s
+      float *Pb = P + (2111 - col - 33 * j0) + (c0 ? 1 : 0);  // bin M - col - 32 s
+      static_for<0, 16>([&](auto ii) {
+        constexpr int i = decltype(ii)::value;
+        const cpx za = z[i];
+        cpx zb;
+        if constexpr (i == 0) zb = c0 ? (j0 ? z[31] : z[0]) : rcv[15];
+        else zb = c0 ? (j0 ? z[31 - i] : z[32 - i]) : rcv[15 - i];
+        const float ex = za.x + zb.x, ey = za.y - zb.y;
+        const float ox = za.y + zb.y, oy = zb.x - za.x;
+        const cpx w = rs_tw[66 * i + 33 * j0 + col];  // W_N^k
+        const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
+        const float xr = ex + wr, xi = ey + wi;
+        const float yr = ex - wr, yi = ey - wi;
+        Pa[66 * i] = fmaf(xr, xr, xi * xi);
+        const float q = fmaf(yr, yr, yi * yi);
+        if constexpr (i == 0) Pb[(c0 && !j0) ? -1 : 0] = q;  // column 0, s = 0: the Nyquist bin
+        else Pb[-66 * i] = q;
+      });
+      if (c0 && !j0) P[M / 2 + 32] = 4.0f * fmaf(z[16].x, z[16].x, z[16].y * z[16].y);
+    }
+    frame_sync<TPF>(fp);  // P complete
+
+    // ---- log-mel row of this frame + running clip max
+    float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
+    if (lanes) {
+      // the filterbank walk of the single-warp kernel over 64 lanes
+      float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
+      const int2 li = lane_s[j];
+      const unsigned fl = (unsigned)li.x;
+      int slot = li.y & 1023;
+      const float *pl = P + 33 * j;
+      const float2 *wl = lw_s + j;
+      float R = 0.0f, Fs = 0.0f, tot = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 32; b++) {
+        const float p = pl[b];
+        const float2 w = wl[b * TPF];
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        if (fl & (1u << b)) {
+          parts[slot++] = make_float2(R, Fs);
+          tot += R + Fs;
+          R = 0.0f;
+          Fs = 0.0f;
+        }
+      }
+      if (j == TPF - 1) {
+        const float p = pl[32];
+        const float2 w = wl[32 * TPF];
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        parts[slot] = make_float2(R, Fs);
+        tot += R + Fs;
+      }
+      if (j == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);  // the empty segments' slot
+      const bool bad = frame_sync_or<TPF>(fp, !isfinite(tot));
+      const int kc = (li.y >> 10) & 63;
+      if (kc) {
+        const int h = j == TPF - 1 ? slot : slot - 1;
+        float2 hv = parts[h];
+        for (int q = 1; q <= kc; q++) {
+          const float2 pv = parts[h + q];
+          hv.x += pv.x;
+          hv.y += pv.y;
+        }
+        parts[h] = hv;
+      }
+      frame_sync<TPF>(fp);
+      for (int m = j; m < nmel; m += TPF) {
+        const int bw = band_s[m];
+        float acc = parts[bw & 4095].x + parts[(bw >> 12) & 4095].y;
+        acc *= 0.25f;
+        if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
+        const float val = db10_frame(acc, a.amin, ref_db);
+        dst[m] = val;
+        vmax = fmaxf(vmax, val);
+      }
+    } else {
+      float chk = 0.0f;  // the frame's non-finite check: this thread's share of the bins
+      for (int k = j; k <= M; k += TPF) chk += P[pad_bin<TPF>(k)];
+      const bool bad = frame_sync_or<TPF>(fp, !isfinite(chk));
+      for (int m = j; m < nmel; m += TPF) {
+        const float acc = 0.25f * mel_dot_pad<TPF>(__ldg(a.mel_info + m), melw, P, bad);
+        const float val = db10_frame(acc, a.amin, ref_db);
+        dst[m] = val;
+        vmax = fmaxf(vmax, val);
+      }
+    }
+  }
+  float m = vmax;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+  if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+}
+
+static cudaError_t launch_warp2(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  using S = W2Shape;
+  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * 34 * (size_t)S::TPF
+                                      : (a.mel_nnz <= S::MEL_SMEM_MAX ? align16(4 * (size_t)a.mel_nnz) : 0);
+  const size_t smem = warp2_fixed_smem() + tables;
+  int per_sm = 1, sms = 148;
+  cudaError_t e =
+      persistent_geometry(reinterpret_cast<const void *>(frame_warp2_kernel), S::THREADS, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = (long long)sms * per_sm;
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  if (grid < 1) return cudaSuccess;
+  frame_warp2_kernel<<<(unsigned)grid, S::THREADS, smem, s>>>(a);
+  if (launched) *launched = (int)grid;
+  return cudaGetLastError();
+}
+
 template <int LOG2N>
 static cudaError_t launch_warp_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using S = WShape<LOG2N>;
@@ -591,6 +911,7 @@ cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, 
     case 9: return launch_warp_t<9>(a, grid_limit, s, launched);
     case 10: return launch_warp_t<10>(a, grid_limit, s, launched);
     case 11: return launch_warp_t<11>(a, grid_limit, s, launched);
+    case 12: return launch_warp2(a, grid_limit, s, launched);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -364,11 +364,14 @@ def test_every_launch_variant_vs_oracle(n_fft):
     (512, 400, 160, "constant"),    # window shorter than n_fft
     (512, 512, 128, "reflect"),
     (256, 256, 64, "constant"),
+    (4096, 4096, 1024, "constant"),  # one frame per warp pair
+    (4096, 4096, 1001, "reflect"),
+    (4096, 3000, 700, "constant"),
 ])
 def test_warp_kernel_uneven_batch_vs_oracle(n_fft, win, hop, pad_mode):
-    """Variant 3 (one warp per frame) on uneven clips: clips shorter than a
-    frame, clips whose start is not 8-byte aligned in the batch buffer, and
-    frames that reach into the padding on both ends."""
+    """Variant 3 (one warp per frame, a warp pair for n_fft 4096) on uneven
+    clips: clips shorter than a frame, clips whose start is not 8-byte aligned
+    in the batch buffer, and frames that reach into the padding on both ends."""
     rng = np.random.default_rng(n_fft + hop)
     lens = [1, 3, n_fft // 2 + 1, n_fft - 1, n_fft + 1, 5 * n_fft + 3] + \
            [int(x) for x in rng.integers(1000, 60000, 5)]
@@ -450,6 +453,11 @@ def test_nonfinite_samples_floor_their_frames(n_fft, hop, n_mels):
     (512, 100, 0.0, None),       # lane tables near their slot limit
     (512, 120, 0.0, None),       # over it: packed rows
     (256, 40, 50.0, None),
+    (4096, 1, 0.0, None),
+    (4096, 128, 0.0, None),
+    (4096, 64, 300.0, 4000.0),
+    (4096, 700, 0.0, None),
+    (4096, 1100, 0.0, None),     # more parts than the lane tables hold: packed rows
 ])
 def test_warp_kernel_filterbank_shapes_vs_oracle(n_fft, n_mels, fmin, fmax):
     """The warp kernel's filterbank walk (parts per lane, segment heads that
@@ -458,16 +466,38 @@ def test_warp_kernel_filterbank_shapes_vs_oracle(n_fft, n_mels, fmin, fmax):
     MFCC bound also bounds the log-mel rows."""
     y = synth.music_clip(4 * SR + 77, SR, seed=n_fft + n_mels)
     n_mfcc = min(n_mels, 32)
-    old = M.tune_get(n_fft)
-    try:
-        M.tune_set(n_fft, 3)
-        got = M.mfcc(y, sr=SR, n_mfcc=n_mfcc, n_fft=n_fft, hop_length=n_fft // 4, n_mels=n_mels,
-                     fmin=fmin, fmax=fmax)
-    finally:
-        M.tune_set(n_fft, old)
     exp = O.mfcc(y, SR, n_mfcc, n_fft, n_fft // 4, n_fft, n_mels, fmin, fmax)
-    assert got.shape == exp.shape
-    assert O.mfcc_rel_error(got, exp) < MFCC_TOL, O.mfcc_rel_error(got, exp)
+    # n_fft 4096: the CTA-tile kernel (variant 2) walks the same tables
+    for v in ((2, 3) if n_fft == 4096 else (3,)):
+        old = M.tune_get(n_fft)
+        try:
+            M.tune_set(n_fft, v)
+            got = M.mfcc(y, sr=SR, n_mfcc=n_mfcc, n_fft=n_fft, hop_length=n_fft // 4, n_mels=n_mels,
+                         fmin=fmin, fmax=fmax)
+        finally:
+            M.tune_set(n_fft, old)
+        assert got.shape == exp.shape
+        assert O.mfcc_rel_error(got, exp) < MFCC_TOL, (v, O.mfcc_rel_error(got, exp))
+
+
+@pytest.mark.parametrize("n_mels", [128, 1100])
+def test_warp_pair_kernel_nonfinite_samples(n_mels):
+    """n_fft 4096 on the warp-pair kernel: non-finite samples floor their
+    frames through the lane walk's check (128 bands) and the packed rows'
+    check (1100 bands)."""
+    y = synth.music_clip(3 * SR, SR, seed=37)
+    y[9000] = np.nan
+    y[40000] = np.inf
+    old = M.tune_get(4096)
+    try:
+        M.tune_set(4096, 3)
+        got = M.mfcc(y, sr=SR, n_mfcc=32, n_fft=4096, hop_length=1024, n_mels=n_mels)
+    finally:
+        M.tune_set(4096, old)
+    with np.errstate(all="ignore"):
+        exp = O.mfcc(y, SR, 32, 4096, 1024, 4096, n_mels)
+    assert got.shape == exp.shape and np.isfinite(got).all()
+    assert O.mfcc_rel_error(got, exp) < MFCC_TOL
 
 
 def test_batch_mixing_short_and_long_clips_matches_single_calls():

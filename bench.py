@@ -647,6 +647,36 @@ def run_reference(args, rank):
     }
 
 
+def kernel_case(args):
+    """One device-resident MFCC plan at another frame size (hop n_fft/4, 128
+    mels, 20 MFCC) over --clips 30 s clips at 22050 Hz, --variant fixed, for
+    kernel profiles: prints the mean plan time over --steps replays."""
+    import torch
+    import metalmom_b200 as M
+    from metalmom_b200 import synth
+    n_fft = args.kernel_case
+    base = synth.music_clip(CLIP_SAMPLES + 997 * args.clips, SR, seed=5)
+    clips = [base[997 * i: 997 * i + CLIP_SAMPLES] for i in range(args.clips)]
+    if args.variant is not None:
+        M.tune_set(n_fft, args.variant)
+    plan = M.Plan([CLIP_SAMPLES] * args.clips, sr=SR, n_fft=n_fft, hop_length=n_fft // 4, n_mels=N_MELS,
+                  n_mfcc=N_MFCC)
+    stream = torch.cuda.Stream()
+    plan.execute_host(clips, stream=stream.cuda_stream)
+    for _ in range(args.warmup):
+        plan.execute(stream=stream.cuda_stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream=stream.cuda_stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    out = {"kernel_case": {"n_fft": n_fft, "hop_length": n_fft // 4, "clips": args.clips,
+                           "variant": M.tune_get(n_fft), "ms_per_step": a.elapsed_time(b) / max(args.steps, 1)}}
+    plan.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -663,7 +693,12 @@ def main():
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--variant", type=int, default=None, help="fixed frame-kernel launch variant (no autotuning)")
     ap.add_argument("--e2e-branch-clips", type=int, default=32)
+    ap.add_argument("--kernel-case", type=int, default=None, metavar="N_FFT",
+                    help="only a device-resident plan at this n_fft (kernel profiles); no bench line")
     args = ap.parse_args()
+    if args.kernel_case is not None:
+        print(json.dumps(kernel_case(args)))
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -376,12 +376,19 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       dft16(e);
       dft16(o);
       cpx *row = fb + l * 33;
+      // W_M^(l (k + 16)) = W_M^(l k) W_M^(16 l): half of the table reads
+      const cpx g16 = tw2[15 * TPF + l];
       static_for<0, 16>([&](auto ki) {
         constexpr int k = decltype(ki)::value;
         const cpx t = tw_const<k, 32>(o[k]);
         cpx lo = cadd(e[k], t), hi = csub(e[k], t);
-        if constexpr (k > 0) lo = cmul(lo, tw2[(k - 1) * TPF + l]);
-        hi = cmul(hi, tw2[(k + 15) * TPF + l]);
+        if constexpr (k > 0) {
+          const cpx tk = tw2[(k - 1) * TPF + l];
+          lo = cmul(lo, tk);
+          hi = cmul(hi, cmul(tk, g16));
+        } else {
+          hi = cmul(hi, g16);
+        }
         row[k] = lo;
         row[k + 16] = hi;
       });
@@ -729,12 +736,18 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       dft16(e);
       dft16(o);
       cpx *row = fb + j * 33;
+      const cpx g16 = tw2[15 * TPF + j];  // W_M^(16 j)
       static_for<0, 16>([&](auto ki) {
         constexpr int k = decltype(ki)::value;
         const cpx tt = tw_const<k, 32>(o[k]);
         cpx lo = cadd(e[k], tt), hi = csub(e[k], tt);
-        if constexpr (k > 0) lo = cmul(lo, tw2[(k - 1) * TPF + j]);
-        hi = cmul(hi, tw2[(k + 15) * TPF + j]);
+        if constexpr (k > 0) {
+          const cpx tk = tw2[(k - 1) * TPF + j];
+          lo = cmul(lo, tk);
+          hi = cmul(hi, cmul(tk, g16));
+        } else {
+          hi = cmul(hi, g16);
+        }
         row[k] = lo;
         row[k + 16] = hi;
       });

@@ -119,3 +119,16 @@ def test_no_gpu_is_reported_not_hidden():
         M.Server()
     with pytest.raises(RuntimeError, match="status -2"):
         M.Plan([4096, 5000], clip_params=[dict(sr=22050), dict(sr=16000, n_fft=512)])
+
+
+def test_untuned_launch_variants():
+    """Before any autotuning: the warp kernels (variant 3) for n_fft 2048 and
+    4096, the CTA-tile kernel (variant 0) for every other size; mm_tune_set
+    validates its arguments and the setting round-trips."""
+    assert [M.tune_get(1 << b) for b in range(4, 16)] == [0] * 7 + [3, 3] + [0] * 3
+    assert lib.mm_tune_set(1000, 0) == -1 and lib.mm_tune_set(2048, 4) == -1 and lib.mm_tune_set(2048, -1) == -1
+    M.tune_set(1024, 2)
+    try:
+        assert M.tune_get(1024) == 2
+    finally:
+        M.tune_set(1024, 0)

@@ -14,9 +14,11 @@ within 60 dB, up to 3e-3 dB for the few values 60-80 dB down that the top_db
 floor keeps (small n_fft, high dynamic range); the reference's float32 path
 rounds the same way.
 
-The draw covers the kernel choices the library makes on its own: the warp
-kernel with lane tables or packed rows, the CTA-tile kernels of every size and
-the tiny direct-DFT kernel.
+The draw covers the kernel choices the library makes on its own (the warp
+kernels for n_fft 2048 and 4096, the CTA-tile kernels of every size, the tiny
+direct-DFT kernel), and each draw runs again with the warp kernels forced for
+n_fft 256..4096 (lane tables or packed rows); sizes and modes without them
+keep their own kernel.
 """
 
 import numpy as np
@@ -48,8 +50,26 @@ def _draw(seed):
                 pad=pad)
 
 
+@pytest.fixture(params=[None, 3], ids=["default", "warp"])
+def variant(request):
+    """The library's own kernel choice, then the warp kernels (launch variant
+    3, n_fft 256..4096) forced for every size that has them."""
+    if request.param is None:
+        yield None
+        return
+    sizes = [1 << b for b in range(4, 16)]
+    old = {n: M.tune_get(n) for n in sizes}
+    for n in sizes:
+        M.tune_set(n, request.param)
+    try:
+        yield request.param
+    finally:
+        for n, v in old.items():
+            M.tune_set(n, v)
+
+
 @pytest.mark.parametrize("seed", range(40))
-def test_random_config_vs_oracle(seed):
+def test_random_config_vs_oracle(seed, variant):
     c = _draw(seed)
     y = synth.music_clip(c["L"], c["sr"], seed=seed)
     pm = O.PAD_REFLECT if c["pad"] == "reflect" else O.PAD_CONSTANT

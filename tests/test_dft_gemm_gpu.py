@@ -67,6 +67,9 @@ class _Dev:
     (512, 512, 128, "reflect"),
     (1024, 1024, 256, "constant"),
     (1024, 600, 200, "reflect"),   # window shorter than n_fft, odd support offset
+    (512, 401, 160, "constant"),   # odd window lengths
+    (1024, 1023, 256, "reflect"),
+    (256, 2, 64, "constant"),      # a two-sample window: one K chunk
 ])
 def test_sizes_and_padding_bf16x3(n_fft, win, hop, pad_mode):
     p = dict(sr=22050, n_fft=n_fft, hop_length=hop, win_length=win, n_mels=64, n_mfcc=20)
@@ -95,3 +98,4 @@ def test_non_finite_input_and_unsupported_sizes():
     assert o.shape == (13, 51)
     with pytest.raises(RuntimeError, match="status -1"):
         M.mfcc_batch([y], dft="bf16x3", sr=22050, n_fft=2048)  # the GEMM forms stop at n_fft 1024
+

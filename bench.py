@@ -585,7 +585,13 @@ def run_ours(args, rank, world, local_rank):
                          "kernel_ms": frame_ms, "dct_ms": dct_ms,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "pipeline_frac": pipe_bytes / (ms_step / 1e3) / 1e9 / hbm,
-                         "fp32_fft_tflops": flops_fft / (frame_ms / 1e3) / 1e12},
+                         "fp32_fft_tflops": flops_fft / (frame_ms / 1e3) / 1e12,
+                         # the kernel's binding roof is compute, not HBM: FFT-form flops
+                         # (2.5 N log2 N per frame) against the FP32 CUDA-core peak, nominal
+                         # (148 SMs x 128 lanes x 2 flop x the sampled max SM clock)
+                         "fp32_peak_tflops_nominal": 148 * 128 * 2 * (peaks.get("sm_max_mhz") or 1965.0) / 1e6,
+                         "fp32_fft_frac_of_nominal": flops_fft / (frame_ms / 1e3) / 1e12
+                         / (148 * 128 * 2 * (peaks.get("sm_max_mhz") or 1965.0) / 1e6)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ke, "branches": plan_io.branches,
                     "api": "Plan.execute_host (mm_plan_execute_host), pinned host buffers",

@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
             const int bin = kb + col / 2 + q;
             if (bin >= kb + nb) break;
             const float p = fmaf(v[2 * q], v[2 * q], v[2 * q + 1] * v[2 * q + 1]);
-            chk += p;
+            chk = fmaf(p, 0.0f, chk);  // NaN iff a bin is not finite
             if (bin < seg_lo || bin >= seg_hi) continue;
             while (cur < nmel && bin >= seg_s[cur + 1].x) finish_seg();
             const float2 w = w2_s[bin];

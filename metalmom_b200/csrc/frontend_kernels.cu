@@ -353,7 +353,7 @@ frontend_kernel(FrontArgs a) {
     constexpr int TW = TPF / 2;
     const bool walk = MODE == MODE_MELDB && a.mel_lane_ok;
     auto pk = [&](int k) { return walk ? k + min(k >> 5, TW - 1) : k; };
-    float chk = 0.0f;  // sum of this thread's |X|^power: non-finite iff one term is
+    float chk = 0.0f;  // sum of this thread's |X|^power * 0: NaN iff one term is not finite
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int k = j + i * TPF;
@@ -361,12 +361,12 @@ frontend_kernel(FrontArgs a) {
       const float y = apply_power<PW>(pb[i], a.power);
       P[pk(k)] = x;
       P[pk(M - k)] = y;
-      chk += x + y;
+      chk = fmaf(x, 0.0f, fmaf(y, 0.0f, chk));
     }
     if (j == 0) {
       const float x = apply_power<PW>(pmid, a.power);
       P[pk(M / 2)] = x;
-      chk += x;
+      chk = fmaf(x, 0.0f, chk);
     }
     const bool bad = frame_sync_or<TPF>(f, !isfinite(chk));
 
@@ -540,7 +540,7 @@ __global__ void __launch_bounds__(128) frontend_tiny_kernel(FrontArgs a, int n_f
         }
       }
       p[k] = apply_power<PW>(re * re + im * im, a.power);
-      if (k < nfreq) chk += p[k];
+      if (k < nfreq) chk = fmaf(p[k], 0.0f, chk);  // NaN iff a bin is not finite
     }
     __syncthreads();
 #pragma unroll

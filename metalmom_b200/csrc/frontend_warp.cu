@@ -19,10 +19,12 @@
 //   and 32-k1 sit in the same lane (TPF < 32); for TPF = 32 the partner lanes
 //   l and 32-l swap the upper 16 registers by shuffle and each takes 16 pairs.
 //
-// Only warp-level synchronisation is used.  The spectrum is kept as |2X|^2
-// (the 1/2 of E and O is not applied) and the mel sums are scaled by 1/4,
-// which is exact in float arithmetic.  The window, the stage-2 twiddles and
-// the mel tables are staged in shared memory once per CTA.
+// Only warp-level synchronisation is used.  The window is staged in shared
+// memory halved (exact in binary floating point), so the real split's
+// E + W O, formed without its factor 1/2, is X itself and the spectrum is
+// |X|^2, bit for bit the values of the unscaled transform divided by 4: a bin
+// overflows float32 only where the reference's |X|^2 does.  The window, the
+// stage-2 twiddles and the mel tables are staged once per CTA.
 #include <math.h>
 
 #include <algorithm>
@@ -268,8 +270,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     const int k1 = i / TPF + 1, j = i - (k1 - 1) * TPF;
     tw2[i] = root_q(twq, 2 * j * k1, N);
   }
-  for (int i = tid; i < N / 4; i += S::THREADS)
-    reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+  for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the header comment
+    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+    reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
+  }
   if constexpr (C == 1)
     for (int i = tid; i < 16 * 32; i += S::THREADS) rs_tw[i] = root_q(twq, (i & 31) + 32 * (i >> 5), N);
   if (lanes) {
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     for (int cc = 0; cc < C; cc++) dft_any<TPF>(v + cc * TPF);
     __syncwarp();  // every lane has read its columns: fb becomes P
 
-    // ---- real split, P[k] = |2 X[k]|^2
+    // ---- real split, P[k] = |X[k]|^2 (the window was halved)
     if constexpr (C == 1) {
       // lanes l and 32-l swap registers 16..31: pair i of lane l is
       // (Z[l + 32 i], Z[M - l - 32 i]) = (v[i], partner's v[31 - i]); lane 0
@@ -499,19 +503,18 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       int slot = li.y & 1023;
       const float *pl = P + 33 * l;
       const float2 *wl = lw_s + l;
-      // Every bin enters both sums (zero weights included; the lane tables
-      // hold finite weights only), so a non-finite bin makes its part
-      // non-finite: `tot` over the parts carries the frame's check.
+      // The frame's non-finite check: `tot` accumulates p * 0 over the lane's
+      // bins (NaN for a NaN or inf bin, and no overflow), then a ballot.
       float R = 0.0f, Fs = 0.0f, tot = 0.0f;
 #pragma unroll
       for (int b = 0; b < 32; b++) {
         const float p = pl[b];
         const float2 w = wl[b * TPF];
+        tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
         if (fl & (1u << b)) {
           parts[slot++] = make_float2(R, Fs);
-          tot += R + Fs;
           R = 0.0f;
           Fs = 0.0f;
         }
@@ -519,10 +522,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       if (l == TPF - 1) {
         const float p = pl[32];
         const float2 w = wl[32 * TPF];
+        tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
         parts[slot] = make_float2(R, Fs);
-        tot += R + Fs;
       }
       const bool bad = (__ballot_sync(FULL, !isfinite(tot)) & gmask) != 0;
       if (l == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);  // the empty segments' slot
@@ -543,7 +546,6 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       for (int m = l; m < nmel; m += TPF) {
         const int bw = band_s[m];
         float acc = parts[bw & 4095].x + parts[(bw >> 12) & 4095].y;
-        acc *= 0.25f;
         if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
         const float val = db10_frame(acc, a.amin, ref_db);
         if (valid) {
@@ -552,11 +554,11 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         }
       }
     } else {
-      float chk = 0.0f;  // the frame's non-finite check: this lane's share of the bins
-      for (int k = l; k <= M; k += TPF) chk += P[pad_bin<TPF>(k)];
+      float chk = 0.0f;  // the frame's non-finite check: this lane's share of the bins, times 0
+      for (int k = l; k <= M; k += TPF) chk = fmaf(P[pad_bin<TPF>(k)], 0.0f, chk);
       const bool bad = (__ballot_sync(FULL, !isfinite(chk)) & gmask) != 0;
       for (int m = l; m < nmel; m += TPF) {
-        const float acc = 0.25f * mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
+        const float acc = mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
         const float val = db10_frame(acc, a.amin, ref_db);
         if (valid) {
           dst[m] = val;
@@ -647,8 +649,10 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
     const int k1 = i / TPF + 1, jj = i - (k1 - 1) * TPF;
     tw2[i] = root_q(twq, 2 * jj * k1, N);
   }
-  for (int i = tid; i < N / 4; i += S::THREADS)
-    reinterpret_cast<float4 *>(win_s)[i] = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+  for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the header comment
+    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+    reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
+  }
   for (int i = tid; i < S::RS; i += S::THREADS) {
     const int s = i / 33, cc = i - 33 * s;
     rs_tw[i] = cc < 32 ? root_q(twq, cc + 32 * s, N) : cpx{0.0f, 0.0f};
@@ -808,7 +812,8 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
     // ---- log-mel row of this frame + running clip max
     float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
     if (lanes) {
-      // the filterbank walk of the single-warp kernel over 64 lanes
+      // the filterbank walk of the single-warp kernel over 64 lanes (and its
+      // non-finite check: p * 0 accumulated over the bins)
       float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
       const int2 li = lane_s[j];
       const unsigned fl = (unsigned)li.x;
@@ -820,11 +825,11 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       for (int b = 0; b < 32; b++) {
         const float p = pl[b];
         const float2 w = wl[b * TPF];
+        tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
         if (fl & (1u << b)) {
           parts[slot++] = make_float2(R, Fs);
-          tot += R + Fs;
           R = 0.0f;
           Fs = 0.0f;
         }
@@ -832,10 +837,10 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       if (j == TPF - 1) {
         const float p = pl[32];
         const float2 w = wl[32 * TPF];
+        tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
         parts[slot] = make_float2(R, Fs);
-        tot += R + Fs;
       }
       if (j == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);  // the empty segments' slot
       const bool bad = frame_sync_or<TPF>(fp, !isfinite(tot));
@@ -854,18 +859,17 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       for (int m = j; m < nmel; m += TPF) {
         const int bw = band_s[m];
         float acc = parts[bw & 4095].x + parts[(bw >> 12) & 4095].y;
-        acc *= 0.25f;
         if (((bw >> 24) & 1) || bad) acc = __int_as_float(0x7fc00000);
         const float val = db10_frame(acc, a.amin, ref_db);
         dst[m] = val;
         vmax = fmaxf(vmax, val);
       }
     } else {
-      float chk = 0.0f;  // the frame's non-finite check: this thread's share of the bins
-      for (int k = j; k <= M; k += TPF) chk += P[pad_bin<TPF>(k)];
+      float chk = 0.0f;  // the frame's non-finite check: this thread's share of the bins, times 0
+      for (int k = j; k <= M; k += TPF) chk = fmaf(P[pad_bin<TPF>(k)], 0.0f, chk);
       const bool bad = frame_sync_or<TPF>(fp, !isfinite(chk));
       for (int m = j; m < nmel; m += TPF) {
-        const float acc = 0.25f * mel_dot_pad<TPF>(__ldg(a.mel_info + m), melw, P, bad);
+        const float acc = mel_dot_pad<TPF>(__ldg(a.mel_info + m), melw, P, bad);
         const float val = db10_frame(acc, a.amin, ref_db);
         dst[m] = val;
         vmax = fmaxf(vmax, val);

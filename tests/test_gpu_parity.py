@@ -500,6 +500,30 @@ def test_warp_pair_kernel_nonfinite_samples(n_mels):
     assert O.mfcc_rel_error(got, exp) < MFCC_TOL
 
 
+def test_large_finite_samples_are_not_flagged_non_finite():
+    """Broadband samples of ~1e17: every bin power is finite (~3e37) although
+    a thread's bins sum past the float32 range.  The frames' non-finite checks
+    accumulate |X|^2 * 0, so no frame is floored as non-finite: mel power and
+    MFCC follow the oracle on the CTA-tile kernel (variant 0) and the warp
+    kernel (variant 3)."""
+    rng = np.random.default_rng(11)
+    y = (rng.standard_normal(2 * SR) * 1e17).astype(np.float32)
+    exp = O.mfcc(y, SR, 20, 2048, 512, 2048, 128)
+    exp_mel = O.melspectrogram(y, SR, 2048, 512, 2048, True, 2.0, 128)
+    assert np.isfinite(exp_mel).all() and exp_mel.max() > 1e35
+    old = M.tune_get(2048)
+    try:
+        for v in (0, 3):
+            M.tune_set(2048, v)
+            got = M.mfcc(y, sr=SR)
+            assert O.mfcc_rel_error(got, exp) < MFCC_TOL, (v, O.mfcc_rel_error(got, exp))
+    finally:
+        M.tune_set(2048, old)
+    mel = M.melspectrogram(y, sr=SR)
+    assert np.isfinite(mel).all()
+    assert np.abs(mel - exp_mel).max() <= 1e-5 * exp_mel.max()
+
+
 def test_batch_mixing_short_and_long_clips_matches_single_calls():
     """Clips of 1 MB and more are uploaded from the caller's buffer, shorter
     ones through pinned staging whose upload spans the whole signal region;

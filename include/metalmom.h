@@ -245,6 +245,10 @@ MM_API int32_t mm_plan_kernel_launches(mm_plan plan);
  * clips' frame counts), before the top_db floor; and clip i's maximum dB. */
 MM_API float* mm_plan_device_mel_db(mm_plan plan);
 MM_API int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float* max_db);
+/* (Any plan.)  Device address of clip i's log-mel rows of the last execution,
+ * frame-major [n_frames_i, n_mels of its group], before the top_db floor;
+ * NULL for an invalid clip. */
+MM_API const float* mm_plan_clip_mel_db(mm_plan plan, int32_t clip);
 /* Replays the captured graph on `stream`. */
 MM_API int32_t mm_plan_execute(mm_plan plan, void* stream);
 /* (Plans of one branch.)  Same kernels launched directly, with CUDA events
@@ -311,6 +315,14 @@ MM_API void mm_server_destroy(mm_server server);
  * whose batch alone exceeds the budget fails with MM_ERR_ALLOC_FAILED. */
 MM_API int32_t mm_server_submit(mm_server server, const float* signal, int64_t length,
                                 const MMFrontEndParams* params, int64_t* request_id);
+/* As mm_server_submit without the copy: the server reads `signal` (length
+ * samples) in place when the request's batch starts.  The caller keeps the
+ * buffer alive and unchanged until the request's result has been taken
+ * (mm_server_poll / mm_server_wait returned other than MM_PENDING) or the
+ * server is destroyed.  From pinned host memory (cudaMallocHost /
+ * cudaHostRegister) the upload runs at full PCIe speed with no host copy. */
+MM_API int32_t mm_server_submit_borrowed(mm_server server, const float* signal, int64_t length,
+                                         const MMFrontEndParams* params, int64_t* request_id);
 /* MM_PENDING while running; otherwise moves the result ([rows, n_frames],
  * free with mm_buffer_free) into *out, or returns the request's error, and
  * forgets the request. */
@@ -331,11 +343,16 @@ MM_API int32_t mm_server_reset_stats(mm_server server);
  * which every GPU that loads the library holds until exit.  Same parameters,
  * sentinels and results as mm_mfcc.  Returns MM_ERR_INVALID_INPUT when the
  * clip's log-mel scratch plus tables exceed that array (about 31 000 frames,
- * 12 minutes at 22050 Hz with hop 512, for n_fft 2048 and 128 mels).  Work is enqueued on `stream` (NULL = the default stream);
- * the call waits once for the filterbank size, so d_out is ready after the
- * stream synchronises.  The first call on each device looks up the array's
- * device address, so make that first call before any stream capture.  Calls
- * share the array: calls whose work overlaps on the GPU race. */
+ * 12 minutes at 22050 Hz with hop 512, for n_fft 2048 and 128 mels).  Work
+ * is enqueued on `stream` (NULL = the default stream); d_out is ready after
+ * the stream synchronises.  The array keeps the tables of the last parameter
+ * set used on the device: a call with a new parameter set builds them there
+ * and waits on `stream` once (for the filterbank size), a call that repeats
+ * the previous parameters enqueues three kernels and does not wait.  The
+ * first call on each device looks up the array's device address, so make
+ * that first call before any stream capture; calls after a device reset are
+ * not supported.  Calls share the array: calls whose work overlaps on the
+ * GPU race. */
 MM_API int32_t mm_mfcc_noalloc(const float* d_signal, int64_t signal_length, int32_t sample_rate,
                                int32_t n_mfcc, int32_t n_fft, int32_t hop_length, int32_t win_length,
                                int32_t n_mels, float f_min, float f_max, int32_t center, float* d_out,

@@ -133,6 +133,14 @@ class Plan:
     def device_mel_db(self) -> int:
         return int(ffi.cast("uintptr_t", lib.mm_plan_device_mel_db(self._plan)))
 
+    def clip_mel_db_ptr(self, clip: int) -> int:
+        """Device address of clip ``clip``'s frame-major log-mel rows (before
+        the top_db floor) of the last execution."""
+        p = lib.mm_plan_clip_mel_db(self._plan, clip)
+        if p == ffi.NULL:
+            raise RuntimeError("no log-mel rows for this clip")
+        return int(ffi.cast("uintptr_t", p))
+
     def clip_max_db(self, clip: int) -> float:
         v = ffi.new("float*")
         st = lib.mm_plan_clip_max_db(self._plan, clip, v)

@@ -41,6 +41,7 @@
 
 #include <algorithm>
 
+#include "async_copy.cuh"
 #include "frame_common.cuh"
 #include "kernels.h"
 
@@ -132,10 +133,6 @@ __global__ void build_dft_basis_kernel(__nv_bfloat16 *img, DftShape s, int win, 
 // ---------------------------------------------------------------------------
 // tcgen05 / mbarrier helpers (inline PTX)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
 // K-major operand, 128-byte swizzle: rows of 128 bytes, 8-row groups 1024
 // bytes apart (stride byte offset), sm_100 descriptor version 1.
 __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
@@ -165,28 +162,6 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t da, uint64_t d
 __device__ __forceinline__ void umma_commit(uint32_t mbar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
                : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t mbar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(mbar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait on an mbarrier phase: false after ~2^22 polls (well over a
-// second), which the caller turns into an error.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++) {
-    if (mbar_try_wait(mbar, parity)) return true;
-    if (it > 64) __nanosleep(64);
-  }
-  return false;
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -271,26 +246,6 @@ __host__ __device__ inline DftSmem dft_smem_layout(const DftShape &s, int n_mels
   p += 16;
   L.total = p + 1024;  // slack to align the base to 1024 bytes
   return L;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-// One arrival that also announces `bytes` of bulk copies completing on the barrier.
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-// 1-D bulk copy global -> shared (no multicast), completing on `bar`.
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
 }
 
 template <int SPLIT>

@@ -11,9 +11,15 @@
 //
 // The array holds kNoallocScratchBytes (16 MiB) on every GPU that loads the
 // library, for as long as the library stays loaded.  Every call shares it and
-// it keeps the previous call's contents; the per-clip maximum is reset on each
-// call.  Two calls whose work overlaps on the GPU (different streams, or
-// different host threads) race on the array.
+// it keeps the previous call's contents: the tables of the last parameter set
+// stay at its start, and the per-clip maximum is reset on each call.  Two
+// calls whose work overlaps on the GPU (different streams, or different host
+// threads) race on the array.
+//
+// Cost per call: the first call with a parameter set (per device) builds the
+// tables into the array and waits once on `stream` for the filterbank size;
+// a call with the same parameters as the device's previous call enqueues one
+// descriptor kernel, the frame kernel and the DCT, and does not wait.
 #include <stdint.h>
 #include <string.h>
 
@@ -29,34 +35,53 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
 
+// What the array's start holds on one device: the tables of one parameter set.
+struct TableKey {
+  int sr = 0, n_fft = 0, win = 0, n_mels = 0, n_mfcc_eff = 0;
+  float fmin = 0.0f, fmax = 0.0f;
+  bool operator==(const TableKey &o) const {
+    return sr == o.sr && n_fft == o.n_fft && win == o.win && n_mels == o.n_mels && n_mfcc_eff == o.n_mfcc_eff &&
+           fmin == o.fmin && fmax == o.fmax;
+  }
+};
+
+struct DeviceState {
+  void *base = nullptr;  // device address of the array (looked up once)
+  bool built = false;
+  TableKey key;
+  mm::DevTables t;
+  size_t used = 0;  // bytes of the array the tables take (256-byte multiple)
+};
+
 std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[kMaxDevices] = {};
+DeviceState g_noalloc_dev[kMaxDevices];
 
 // Device address of the scratch array for the current device.  The host-side
-// name `g_noalloc_scratch` is only a stand-in; the address has to be looked up
-// once per device, with that device current.
-int noalloc_scratch(char **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return mm::cuda_status(e);
-  if (dev < 0 || dev >= kMaxDevices) return MM_ERR_INTERNAL;
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+// name `g_noalloc_scratch` is only a stand-in: the address is looked up once
+// per device, at that device's first call, with the device current.  (A
+// device reset unloads the module; calls after one are not supported.)  The
+// caller holds g_noalloc_mu.
+int noalloc_scratch(int dev, char **out) {
+  DeviceState &d = g_noalloc_dev[dev];
+  if (!d.base) {
     void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
       return MM_ERR_INTERNAL;
     }
-    g_noalloc_ptr[dev] = p;
+    d.base = p;
+    d.built = false;
   }
-  *out = static_cast<char *>(g_noalloc_ptr[dev]);
+  *out = static_cast<char *>(d.base);
   return MM_OK;
 }
 
-// Single-clip descriptors written on the device (no host copies).
+// Single-clip descriptors and the reset clip maximum, written on the device
+// (no host copies).
 __global__ void noalloc_desc_kernel(mm::ClipDesc *cd, long long sig_off, long long length, int n_frames,
-                                    int *tile_clip, int tiles, int *dct_clip, int *dct_first, int dct_tiles) {
+                                    int *tile_clip, int tiles, int *dct_clip, int *dct_first, int dct_tiles,
+                                    unsigned *clip_max, unsigned max_init) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
     cd->sig_off = sig_off;
@@ -65,6 +90,7 @@ __global__ void noalloc_desc_kernel(mm::ClipDesc *cd, long long sig_off, long lo
     cd->out_off = 0;
     cd->n_frames = n_frames;
     cd->tile_base = 0;
+    *clip_max = max_init;
   }
   for (int k = i; k < tiles; k += gridDim.x * blockDim.x) tile_clip[k] = 0;
   for (int k = i; k < dct_tiles; k += gridDim.x * blockDim.x) {
@@ -119,16 +145,42 @@ extern "C" MM_API int32_t mm_mfcc_noalloc(const float *d_signal, int64_t signal_
                              up256(sizeof(float) * (size_t)T * (size_t)n_mels);
   if (batch_bytes >= kNoallocScratchBytes) return MM_ERR_INVALID_INPUT;  // clip too long for the scratch
 
-  char *base = nullptr;
-  if ((st = noalloc_scratch(&base)) != MM_OK) return st;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (dev < 0 || dev >= kMaxDevices) return MM_ERR_INTERNAL;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  TableKey key;
+  key.sr = g.sr;
+  key.n_fft = g.n_fft;
+  key.win = g.win;
+  key.n_mels = g.n_mels;
+  key.n_mfcc_eff = g.n_mfcc_eff;
+  key.fmin = g.fmin;
+  key.fmax = g.fmax;
 
+  char *base = nullptr;
   DevTables t;
   size_t used = 0;
-  cudaError_t e = build_tables_at(t, base, kNoallocScratchBytes - batch_bytes, &used, g.sr, g.n_fft, g.win,
-                                  g.n_mels, g.fmin, g.fmax, g.n_mfcc_eff, 0, s);
-  if (e == cudaErrorMemoryAllocation) return MM_ERR_INVALID_INPUT;  // tables too large for the scratch
-  if (e != cudaSuccess) return cuda_status(e);
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if ((st = noalloc_scratch(dev, &base)) != MM_OK) return st;
+    DeviceState &d = g_noalloc_dev[dev];
+    if (!(d.built && d.key == key)) {
+      // (Re)build this parameter set's tables at the array's start; the
+      // previous set's tables are gone from here on.
+      d.built = false;
+      e = build_tables_at(d.t, base, kNoallocScratchBytes, &d.used, g.sr, g.n_fft, g.win, g.n_mels, g.fmin,
+                          g.fmax, g.n_mfcc_eff, 0, s);
+      if (e == cudaErrorMemoryAllocation) return MM_ERR_INVALID_INPUT;  // tables too large for the scratch
+      if (e != cudaSuccess) return cuda_status(e);
+      d.key = key;
+      d.built = true;
+    }
+    t = d.t;
+    used = d.used;
+  }
+  if (used + batch_bytes > kNoallocScratchBytes) return MM_ERR_INVALID_INPUT;  // clip too long for the scratch
 
   char *p = base + used;
   ClipDesc *cd = reinterpret_cast<ClipDesc *>(p);
@@ -150,9 +202,8 @@ extern "C" MM_API int32_t mm_mfcc_noalloc(const float *d_signal, int64_t signal_
 
   const int nb = std::max(1, std::min(1024, (std::max(tiles, dct_tiles) + 255) / 256));
   noalloc_desc_kernel<<<nb, 256, 0, s>>>(cd, sig_off, signal_length, (int)T, tile_clip, tiles, dct_clip,
-                                         dct_first, dct_tiles);
+                                         dct_first, dct_tiles, clip_max, encode_max_init());
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
-  if ((e = launch_fill_u32(clip_max, encode_max_init(), 1, s)) != cudaSuccess) return cuda_status(e);
 
   FrontArgs a;
   a.signal = sig_base;

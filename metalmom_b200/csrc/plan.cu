@@ -294,6 +294,14 @@ float *mm_plan_device_mel_db(mm_plan plan) {
   return (p && p->subs.size() == 1) ? p->subs[0].b.meldb : nullptr;
 }
 
+const float *mm_plan_clip_mel_db(mm_plan plan, int32_t clip) {
+  Plan *p = as_plan(plan);
+  if (!clip_ok(p, clip)) return nullptr;
+  const Sub &s = p->subs[p->where[clip].first];
+  if (s.g.mode != MODE_MELDB || !s.b.meldb) return nullptr;
+  return s.b.meldb + s.L.clips[p->where[clip].second].frame_off * (long long)s.g.n_mels;
+}
+
 int32_t mm_plan_clip_max_db(mm_plan plan, int32_t clip, float *max_db) {
   Plan *p = as_plan(plan);
   if (!clip_ok(p, clip) || !max_db) return MM_ERR_INVALID_INPUT;

@@ -57,6 +57,21 @@ class PinnedPool {
     while ((size_t(1) << c) < bytes) c++;
     return c;
   }
+  // Pins `bytes` (whole chunks, within the cap) up front, so that serving
+  // does not stop in cudaMallocHost (tens of milliseconds per chunk, under a
+  // driver lock that the scheduler's launches wait on) until that is used up.
+  cudaError_t reserve(size_t bytes) {
+    std::lock_guard<std::mutex> lk(mu_);
+    while (spare_.size() * kChunk < bytes && total_ + kChunk <= cap_) {
+      char *p = nullptr;
+      cudaError_t e = cudaMallocHost(&p, kChunk);
+      if (e != cudaSuccess) return e;
+      chunks_.push_back(p);
+      spare_.push_back(p);
+      total_ += kChunk;
+    }
+    return cudaSuccess;
+  }
   float *get(size_t bytes, int *cls) {
     const int c = size_class(bytes);
     const size_t sz = size_t(1) << c;
@@ -79,14 +94,19 @@ class PinnedPool {
       return reinterpret_cast<float *>(p);
     }
     if (left_ < sz) {
-      if (total_ + kChunk > cap_) return nullptr;
       char *p = nullptr;
-      if (cudaMallocHost(&p, kChunk) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
+      if (!spare_.empty()) {  // a chunk pinned at creation
+        p = spare_.back();
+        spare_.pop_back();
+      } else {
+        if (total_ + kChunk > cap_) return nullptr;
+        if (cudaMallocHost(&p, kChunk) != cudaSuccess) {
+          cudaGetLastError();
+          return nullptr;
+        }
+        chunks_.push_back(p);
+        total_ += kChunk;
       }
-      chunks_.push_back(p);
-      total_ += kChunk;
       cur_ = p;
       left_ = kChunk;
     }
@@ -103,9 +123,13 @@ class PinnedPool {
  private:
   std::mutex mu_;
   std::vector<char *> chunks_;
+  std::vector<char *> spare_;  // reserved chunks not carved yet
   std::vector<char *> free_[64];
   char *cur_ = nullptr;
   size_t left_ = 0, total_ = 0, cap_;
+
+ public:
+  size_t cap() const { return cap_; }
 };
 
 struct Request {
@@ -114,7 +138,8 @@ struct Request {
   long long length = 0;
   float *pin = nullptr;      // samples in a pinned block (pin_cls = its size class) ...
   int pin_cls = 0;
-  std::vector<float> signal;  // ... or, when the pinned pool is full, a pageable copy
+  std::vector<float> signal;  // ... or, when the pinned pool is full, a pageable copy ...
+  const float *borrowed = nullptr;  // ... or the caller's own buffer (mm_server_submit_borrowed)
   float *result = nullptr;  // malloc'd [rows x frames], handed to the caller
   long long rows = 0, frames = 0;
   int state = REQ_PENDING;
@@ -129,6 +154,9 @@ struct Slot {
   cudaStream_t stream = nullptr;
   char *pinned = nullptr;
   size_t pinned_bytes = 0;
+  // staging outgrown while serving: freed at destroy (cudaFreeHost would
+  // synchronise the device in the middle of other batches)
+  std::vector<char *> retired;
   // current batch
   bool busy = false;
   std::atomic<bool> finished{false};
@@ -165,6 +193,7 @@ struct Server {
   double launch_ms = 0.0, finish_ms = 0.0;  // scheduler host time per phase
   std::vector<double> lat_ms;
 
+  size_t pool_cap() const { return pool->cap(); }
   void run();
   bool admit_one(std::unique_lock<std::mutex> &lk);
   void finish(Slot *s);
@@ -263,11 +292,14 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
     slot->out_bytes = sizeof(float) * (size_t)slot->L.out_elems;
     const size_t host_need = std::max(slot->desc_bytes, slot->out_bytes) + 256;
     if (host_need > slot->pinned_bytes) {
-      if (slot->pinned) cudaFreeHost(slot->pinned);
-      slot->pinned = nullptr;
-      slot->pinned_bytes = 0;
-      e = cudaMallocHost(&slot->pinned, host_need + host_need / 4);
-      if (e == cudaSuccess) slot->pinned_bytes = host_need + host_need / 4;
+      const size_t grow = std::max(host_need + host_need / 4, 2 * slot->pinned_bytes);
+      char *p = nullptr;
+      e = cudaMallocHost(&p, grow);
+      if (e == cudaSuccess) {
+        if (slot->pinned) slot->retired.push_back(slot->pinned);
+        slot->pinned = p;
+        slot->pinned_bytes = grow;
+      }
     }
     if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&slot->arena, bytes, mempool, slot->stream);
     if (e == cudaSuccess) {
@@ -276,7 +308,8 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
       DevBatch b;
       carve_arena(g, slot->L, slot->arena, b);
       for (size_t i = 0; i < take.size() && e == cudaSuccess; i++) {
-        const float *src = take[i]->pin ? take[i]->pin : take[i]->signal.data();
+        const float *src = take[i]->pin ? take[i]->pin
+                           : take[i]->borrowed ? take[i]->borrowed : take[i]->signal.data();
         e = cudaMemcpyAsync(b.signal + slot->L.clips[i].sig_off, src, sizeof(float) * (size_t)take[i]->length,
                             cudaMemcpyHostToDevice, slot->stream);
       }
@@ -345,6 +378,7 @@ void Server::finish(Slot *s) {
   for (Request *r : s->reqs) {  // the samples are on the device (or the batch failed)
     if (r->pin) pool->put(r->pin, r->pin_cls);
     r->pin = nullptr;
+    r->borrowed = nullptr;
     std::vector<float>().swap(r->signal);
   }
   if (s->arena) cudaFreeAsync(s->arena, s->stream);
@@ -390,6 +424,56 @@ int32_t deliver(Server *srv, Request *r, MMBuffer *out) {
 
 }  // namespace
 
+namespace {
+// Queue one request: copy the samples into the pinned pool (or a pageable
+// copy), or, when `borrow` is set, keep the caller's pointer.
+int32_t submit_one(Server *srv, const float *signal, int64_t length, const MMFrontEndParams *params,
+                   int64_t *request_id, bool borrow) {
+  if (!srv || !signal || length <= 0 || !request_id) return MM_ERR_INVALID_INPUT;
+  Request *r = new (std::nothrow) Request();
+  if (!r) return MM_ERR_ALLOC_FAILED;
+  int st = resolve_frontend(params, r->g);
+  if (st == MM_OK && (r->g.n_mfcc_eff <= 0 || frame_count(length, r->g.n_fft, r->g.hop, r->g.center) == 0))
+    st = MM_ERR_INVALID_INPUT;  // nothing to compute: callers use mm_mfcc for empty shapes
+  if (st != MM_OK) {
+    delete r;
+    return st;
+  }
+  r->length = length;
+  if (borrow) {
+    r->borrowed = signal;
+  } else {
+    r->pin = srv->pool->get(sizeof(float) * (size_t)length, &r->pin_cls);
+    if (r->pin) {
+      memcpy(r->pin, signal, sizeof(float) * (size_t)length);
+    } else {
+      try {
+        r->signal.assign(signal, signal + length);
+      } catch (...) {
+        delete r;
+        return MM_ERR_ALLOC_FAILED;
+      }
+    }
+  }
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    if (srv->stop) {
+      if (r->pin) srv->pool->put(r->pin, r->pin_cls);
+      delete r;
+      return MM_ERR_INVALID_INPUT;
+    }
+    r->id = srv->next_id++;
+    srv->reqs[r->id] = r;
+    srv->pending.push_back(r);
+    srv->submitted++;
+    *request_id = r->id;
+  }
+  srv->cv.notify_all();
+  return MM_OK;
+}
+}  // namespace
+
 extern "C" {
 
 mm_server mm_server_create(const MMServerConfig *cfg, int32_t *status) {
@@ -424,15 +508,28 @@ mm_server mm_server_create(const MMServerConfig *cfg, int32_t *status) {
     e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     srv->slots.push_back(s);
     if (e == cudaSuccess) {  // descriptors + results of a batch; grows if ever needed
-      s->pinned_bytes = size_t(8) << 20;
+      s->pinned_bytes = size_t(64) << 20;
       e = cudaMallocHost(&s->pinned, s->pinned_bytes);
     }
+  }
+  // Pinned host blocks and device arenas reserved up front: the first
+  // minutes of serving then never wait on cudaMallocHost or on the device
+  // pool growing (both only grow later, past these sizes).
+  if (e == cudaSuccess)
+    e = srv->pool->reserve(std::min<size_t>(size_t(1) << 30, srv->pool_cap()));
+  if (e == cudaSuccess) {
+    void *warm = nullptr;
+    const size_t dev_reserve = std::min<size_t>(srv->budget, size_t(4) << 30);
+    e = cudaMallocFromPoolAsync(&warm, dev_reserve, srv->mempool, srv->slots[0]->stream);
+    if (e == cudaSuccess) e = cudaFreeAsync(warm, srv->slots[0]->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(srv->slots[0]->stream);
   }
   if (e != cudaSuccess) {
     cudaGetLastError();
     for (Slot *s : srv->slots) {
       if (s->stream) cudaStreamDestroy(s->stream);
       if (s->pinned) cudaFreeHost(s->pinned);
+      for (char *r : s->retired) cudaFreeHost(r);
       delete s;
     }
     if (srv->mempool) cudaMemPoolDestroy(srv->mempool);
@@ -466,6 +563,7 @@ void mm_server_destroy(mm_server server) {
       cudaStreamDestroy(s->stream);
     }
     if (s->pinned) cudaFreeHost(s->pinned);
+    for (char *r : s->retired) cudaFreeHost(r);
     delete s;
   }
   for (auto &kv : srv->reqs) {
@@ -479,45 +577,12 @@ void mm_server_destroy(mm_server server) {
 
 int32_t mm_server_submit(mm_server server, const float *signal, int64_t length, const MMFrontEndParams *params,
                          int64_t *request_id) {
-  Server *srv = static_cast<Server *>(server);
-  if (!srv || !signal || length <= 0 || !request_id) return MM_ERR_INVALID_INPUT;
-  Request *r = new (std::nothrow) Request();
-  if (!r) return MM_ERR_ALLOC_FAILED;
-  int st = resolve_frontend(params, r->g);
-  if (st == MM_OK && (r->g.n_mfcc_eff <= 0 || frame_count(length, r->g.n_fft, r->g.hop, r->g.center) == 0))
-    st = MM_ERR_INVALID_INPUT;  // nothing to compute: callers use mm_mfcc for empty shapes
-  if (st != MM_OK) {
-    delete r;
-    return st;
-  }
-  r->length = length;
-  r->pin = srv->pool->get(sizeof(float) * (size_t)length, &r->pin_cls);
-  if (r->pin) {
-    memcpy(r->pin, signal, sizeof(float) * (size_t)length);
-  } else {
-    try {
-      r->signal.assign(signal, signal + length);
-    } catch (...) {
-      delete r;
-      return MM_ERR_ALLOC_FAILED;
-    }
-  }
-  r->t_submit = Clock::now();
-  {
-    std::lock_guard<std::mutex> lk(srv->mu);
-    if (srv->stop) {
-      if (r->pin) srv->pool->put(r->pin, r->pin_cls);
-      delete r;
-      return MM_ERR_INVALID_INPUT;
-    }
-    r->id = srv->next_id++;
-    srv->reqs[r->id] = r;
-    srv->pending.push_back(r);
-    srv->submitted++;
-    *request_id = r->id;
-  }
-  srv->cv.notify_all();
-  return MM_OK;
+  return submit_one(static_cast<Server *>(server), signal, length, params, request_id, false);
+}
+
+int32_t mm_server_submit_borrowed(mm_server server, const float *signal, int64_t length,
+                                  const MMFrontEndParams *params, int64_t *request_id) {
+  return submit_one(static_cast<Server *>(server), signal, length, params, request_id, true);
 }
 
 int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer *out) {

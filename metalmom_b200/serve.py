@@ -28,6 +28,7 @@ class Server:
         cfg.max_batch_clips = int(max_batch_clips)
         cfg.max_inflight = int(max_inflight)
         st = ffi.new("int32_t*")
+        self._borrowed = {}
         self._srv = lib.mm_server_create(cfg, st)
         if self._srv == ffi.NULL:
             raise RuntimeError(f"mm_server_create failed with status {st[0]}")
@@ -42,12 +43,27 @@ class Server:
             raise RuntimeError(f"mm_server_submit failed with status {st}")
         return int(rid[0])
 
+    def submit_borrowed(self, y, **params) -> int:
+        """Queue one clip without copying it: ``y`` (a contiguous float32
+        array, ideally in pinned memory) is read in place when its batch
+        starts, and is held here until its result is taken."""
+        if not (isinstance(y, np.ndarray) and y.dtype == np.float32 and y.flags.c_contiguous):
+            raise ValueError("submit_borrowed needs a contiguous float32 array")
+        p = frontend_params(**params)
+        rid = ffi.new("int64_t*")
+        st = lib.mm_server_submit_borrowed(self._srv, ffi.cast("const float*", y.ctypes.data), len(y), p, rid)
+        if st != 0:
+            raise RuntimeError(f"mm_server_submit_borrowed failed with status {st}")
+        self._borrowed[int(rid[0])] = y
+        return int(rid[0])
+
     def poll(self, rid: int):
         """The result if the request is done, else None."""
         out = ffi.new("MMBuffer*")
         st = lib.mm_server_poll(self._srv, rid, out)
         if st == PENDING:
             return None
+        self._borrowed.pop(rid, None)
         if st != 0:
             raise RuntimeError(f"request {rid} failed with status {st}")
         return buffer_to_numpy(out)
@@ -58,6 +74,7 @@ class Server:
         st = lib.mm_server_wait(self._srv, rid, int(timeout_ms), out)
         if st == PENDING:
             raise TimeoutError(f"request {rid} not done after {timeout_ms} ms")
+        self._borrowed.pop(rid, None)
         if st != 0:
             raise RuntimeError(f"request {rid} failed with status {st}")
         return buffer_to_numpy(out)
@@ -76,6 +93,7 @@ class Server:
         if getattr(self, "_srv", None) is not None and self._srv != ffi.NULL:
             lib.mm_server_destroy(self._srv)
         self._srv = None
+        self._borrowed = {}
 
     def __enter__(self):
         return self

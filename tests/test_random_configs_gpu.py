@@ -6,13 +6,13 @@ mm_mfcc (MFCC within 1e-4 of max |c|) and mm_mel_spectrogram through the C
 ABI, and the batched entry point with the clip in a mixed batch (bitwise
 equal to the single call).
 
-Mel-dB tolerance: 1e-3 dB for values within 60 dB of the clip's maximum,
-1e-2 dB below that.  The float32 FFT's rounding is absolute (a fraction of
-the frame's largest bins), so its dB error grows with the distance below the
-maximum: measured on these draws, <= 4.3e-5 dB within 40 dB, <= 4.1e-4 dB
-within 60 dB, up to 3e-3 dB for the few values 60-80 dB down that the top_db
-floor keeps (small n_fft, high dynamic range); the reference's float32 path
-rounds the same way.
+Mel-dB tolerance (``dbcheck.check_db``): 1e-3 dB for values within 60 dB of
+the clip's maximum; 60-70 and 70-80 dB below it, no worse than FACTOR times
+the error of the reference's own float32 path (``oracle/refcpu.c``) on the
+same draw and distance bin, or 1e-3 dB when that is larger.  The float32
+FFT's rounding is absolute (a fraction of the frame's largest bins), so its dB
+error grows with the distance below the maximum, in the reference's float32
+path as on the GPU.
 
 The draw covers the kernel choices the library makes on its own (the warp
 kernels for n_fft 2048 and 4096, the CTA-tile kernels of every size, the tiny
@@ -25,13 +25,13 @@ import numpy as np
 import pytest
 
 import metalmom_b200 as M
+from dbcheck import check_db
 from metalmom_b200 import synth
-from oracle import oracle as O
+from oracle import oracle as O, refcpu
 
 pytestmark = pytest.mark.gpu
 
 MFCC_TOL = 1e-4
-DB_TOL = 1e-3
 
 
 def _draw(seed):
@@ -86,10 +86,9 @@ def test_random_config_vs_oracle(seed, variant):
         got_db = O.power_to_db(np.asarray(mel, np.float64), 1.0, 1e-10, 80.0)
         exp_db = O.mel_db(y, c["sr"], c["n_fft"], c["hop"], c["win"], True, c["n_mels"], c["fmin"], c["fmax"])
         if exp_db.size:
-            near = exp_db >= exp_db.max() - 60.0
-            err = np.abs(got_db - exp_db)
-            assert err[near].max() < DB_TOL, (c, err[near].max())
-            assert err.max() < 10 * DB_TOL, (c, err.max())
+            _, ref_db = refcpu.mfcc(y, c["sr"], c["n_mfcc"], c["n_fft"], c["hop"], c["win"], c["n_mels"], c["fmin"],
+                                    c["fmax"] or 0.0, True, want_mel_db=True)
+            check_db(got_db, exp_db, ref_db, c)
     # batched, with the padding mode of the draw, next to a clip of another length
     other = synth.music_clip(c["L"] // 3 + 7, c["sr"], seed=seed + 1000)
     bkw = dict(kw, n_mfcc=c["n_mfcc"], pad_mode=c["pad"])

@@ -128,3 +128,24 @@ def test_poll_and_invalid_requests():
         assert out is not None and out.shape == (20, 44)
         with pytest.raises(RuntimeError):
             srv.poll(rid)  # delivered requests are forgotten
+
+
+def test_borrowed_submits_equal_copied_submits():
+    """mm_server_submit_borrowed reads the caller's (here pinned) buffers in
+    place: the results are bitwise those of copied submits."""
+    import torch
+    reqs = _requests(12, seed=7)
+    total = sum(len(y) for y, _ in reqs)
+    buf = torch.empty(total, dtype=torch.float32).pin_memory().numpy()
+    views, off = [], 0
+    for y, _ in reqs:
+        views.append(buf[off:off + len(y)])
+        views[-1][:] = y
+        off += len(y)
+    with M.Server(max_inflight=2, max_batch_clips=4) as srv:
+        a = [srv.submit(y, **g) for y, g in reqs]
+        b = [srv.submit_borrowed(v, **g) for v, (_, g) in zip(views, reqs)]
+        ra = [srv.result(i) for i in a]
+        rb = [srv.result(i) for i in b]
+    for x, y in zip(ra, rb):
+        np.testing.assert_array_equal(x, y)

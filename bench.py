@@ -491,6 +491,8 @@ def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
     out = {"workload": f"{n_clips} clips, lengths U[1,120] s, per-clip group from sr {{22050, 44100}} x "
                        "n_fft {1024, 2048, 4096} (hop n_fft/4) x mels {64, 128}, 20 MFCC",
            "audio_hours": hours, "ms_per_step": ms, "audio_hours_per_s": hours / (ms / 1e3),
+           "samples_per_s": sum(len(c) for c in clips) / (ms / 1e3),
+           "frames_per_s": sum(plan.frames) / (ms / 1e3),
            "groups": len({tuple(sorted(g.items())) for g in params}), "branches": plan.branches,
            "gpu_launches_per_step": plan.kernel_launches, "tuned_variant_per_n_fft": tuned,
            "timing": "CUDA events around graph replays, inputs resident (> L2)",
@@ -729,6 +731,8 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": K * plan.kernel_launches,
             "one_clip_per_launch": per_clip,
+            "samples_per_s": world * sum(lengths) / (ms_step / 1e3),
+            "frames_per_s": world * T_total / (ms_step / 1e3),
             "batched_vs_one_clip": {"device": value / world / per_clip["device_value"],
                                     "e2e": e2e_value / world / per_clip["e2e_value"]},
             "autotune": {"variant": tune["best"], "variant_ms": tune["ms"],

@@ -25,7 +25,6 @@
 #include <mutex>
 #include <tuple>
 
-#include "async_copy.cuh"
 #include "fft_radix.cuh"
 #include "frame_common.cuh"
 #include "kernels.h"
@@ -1617,167 +1616,6 @@ __global__ void __launch_bounds__(256, 3) dct_fold_kernel(DctArgs a) {
   }
 }
 
-// 128 bands, rows brought in by the Tensor Memory Accelerator: a DCT tile's
-// rows (64 consecutive frames of one clip) are one contiguous 32 KB run of
-// the frame-major log-mel buffer, so one 1-D bulk copy (cp.async.bulk, no
-// multicast) moves it into a two-slot shared-memory ring, completing on the
-// slot's mbarrier, while the CTA works on the other slot.  Threads then floor
-// and fold the rows out of the slot into the bank-padded tile and run the
-// product of dct_fold_kernel.  No thread issues a global load for the rows,
-// so the kernel keeps ~64 KB per CTA in flight and runs at the HBM bandwidth
-// instead of the latency of register prefetches.  Every wait is bounded: a
-// wait that runs out sets *a.err, and the CTA waits (bounded) for its own
-// copies still in flight before it returns.
-constexpr int kDctBulkStages = 2;
-constexpr uint32_t kDctBulkSlot = kDctTile * 128 * 4;
-
-__host__ __device__ inline size_t dct_bulk_smem(int kq) {
-  return size_t(kDctBulkStages) * kDctBulkSlot + sizeof(float) * ((size_t)kDctTile * dct_row_stride(128)) +
-         sizeof(float) * (size_t)4 * kq * 64 + 8 * kDctBulkStages + 128;
-}
-
-template <int KQ>
-__global__ void __launch_bounds__(256, 2) dct_bulk_kernel(DctArgs a) {
-  constexpr int NM = 128, H = NM / 2, H4 = H / 4;
-  constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ __align__(128) unsigned char dbk_raw[];
-  const uint32_t raw = smem_u32(dbk_raw);
-  unsigned char *sm = dbk_raw + (((raw + 127u) & ~127u) - raw);
-  unsigned char *ring = sm;                                                  // [stages][64 rows x 512 B]
-  float *tile = reinterpret_cast<float *>(sm + kDctBulkStages * kDctBulkSlot);  // [64][stride]: e | o
-  const int stride = dct_row_stride(NM);
-  float *bas = tile + kDctTile * stride;                                     // [4*KQ][H]
-  const uint32_t bar0 = smem_u32(bas + 4 * KQ * H);                          // full[stages]
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int fr = tid & (kDctTile - 1), kg = tid / kDctTile;
-  auto coef = [](int g, int q) { return g < 2 ? 2 * (KQ * g + q) : 2 * (KQ * (g - 2) + q) + 1; };
-  const int G = gridDim.x;
-  // bytes of tile ti's rows and their address (16-byte aligned: rows are 512 B)
-  auto tile_src = [&](int ti, uint32_t *bytes) {
-    const int c = __ldg(a.tile_clip + ti);
-    const ClipDesc cd = load_clip(a.clips + c);
-    const int tf = __ldg(a.tile_first + ti);
-    *bytes = (uint32_t)min(kDctTile, cd.n_frames - tf) * (uint32_t)(NM * 4);
-    return a.mel_db + (cd.frame_off + tf) * (long long)NM;
-  };
-  if (tid == 0) {
-    for (int st = 0; st < kDctBulkStages; st++) mbar_init(bar0 + 8u * st, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (int st = 0; st < kDctBulkStages; st++) {
-      const int ti = blockIdx.x + st * G;
-      if (ti < a.total_tiles) {
-        uint32_t bytes;
-        const float *src = tile_src(ti, &bytes);
-        mbar_expect_tx(bar0 + 8u * st, bytes);
-        bulk_g2s(smem_u32(ring + st * kDctBulkSlot), src, bytes, bar0 + 8u * st);
-      }
-    }
-  }
-  for (int i = tid; i < 4 * KQ * H; i += 256) {
-    const int row = i / H, n = i - row * H;
-    const int k = coef(row / KQ, row % KQ);
-    bas[i] = k < a.n_mfcc ? __ldg(a.basis + (long long)k * NM + n) : 0.0f;
-  }
-  __syncthreads();
-  const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * H);
-  const float4 *trow = reinterpret_cast<const float4 *>(tile + fr * stride + (kg < 2 ? 0 : H));
-  int it = 0;
-  bool failed = false;
-  for (int ti = blockIdx.x; ti < a.total_tiles; ti += G, it++) {
-    const int st = it % kDctBulkStages;
-    const uint32_t full = bar0 + 8u * st;
-    const bool ok = mbar_wait_bounded(full, (uint32_t)(it / kDctBulkStages) & 1u);
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
-    }
-    const DctTileMeta cur = dct_tile_meta(a, ti);
-    const float4 *slot = reinterpret_cast<const float4 *>(ring + st * kDctBulkSlot);
-#pragma unroll
-    for (int v = 0; v < kDctTile / 8; v++) {
-      const int r = warp + 8 * v;  // warp-uniform
-      float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (r < cur.nt) {
-        x = slot[r * (NM / 4) + lane];
-        x.x = vthr(x.x, cur.thr);
-        x.y = vthr(x.y, cur.thr);
-        x.z = vthr(x.z, cur.thr);
-        x.w = vthr(x.w, cur.thr);
-      }
-      float4 y;
-      y.x = __shfl_xor_sync(FULL, x.x, 31);
-      y.y = __shfl_xor_sync(FULL, x.y, 31);
-      y.z = __shfl_xor_sync(FULL, x.z, 31);
-      y.w = __shfl_xor_sync(FULL, x.w, 31);
-      float4 f;
-      int pos;
-      if (lane < 16) {  // e over chunk lane: x[4l + t] + x[N - 1 - 4l - t]
-        f = make_float4(x.x + y.w, x.y + y.z, x.z + y.y, x.w + y.x);
-        pos = lane;
-      } else {  // o over chunk 31 - l: mirror chunk (from lane 31 - l) minus this one reversed
-        f = make_float4(y.x - x.w, y.y - x.z, y.z - x.y, y.w - x.x);
-        pos = H4 + 31 - lane;
-      }
-      *reinterpret_cast<float4 *>(tile + r * stride + 4 * pos) = f;
-    }
-    __syncthreads();  // the slot is consumed and the tile complete
-    if (tid == 0) {   // refill the slot with the tile after next
-      const int nti = ti + kDctBulkStages * G;
-      if (nti < a.total_tiles) {
-        uint32_t bytes;
-        const float *src = tile_src(nti, &bytes);
-        fence_proxy_async_smem();  // the slot's reads above come before the copy's writes
-        mbar_expect_tx(full, bytes);
-        bulk_g2s(smem_u32(ring + st * kDctBulkSlot), src, bytes, full);
-      }
-    }
-    float acc[KQ];
-#pragma unroll
-    for (int q = 0; q < KQ; q++) acc[q] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < H4; j++) {
-      const float4 d = trow[j];
-#pragma unroll
-      for (int q = 0; q < KQ; q++) {
-        const float4 b = brow[q * H4 + j];
-        acc[q] = fmaf(b.x, d.x, acc[q]);
-        acc[q] = fmaf(b.y, d.y, acc[q]);
-        acc[q] = fmaf(b.z, d.z, acc[q]);
-        acc[q] = fmaf(b.w, d.w, acc[q]);
-      }
-    }
-    if (fr < cur.nt) {
-#pragma unroll
-      for (int q = 0; q < KQ; q++) {
-        const int k = coef(kg, q);
-        if (k < a.n_mfcc) a.out[cur.out_off + (long long)k * cur.T + cur.tf + fr] = acc[q];
-      }
-    }
-    __syncthreads();  // the tile is read before the next one is folded into it
-  }
-  if (failed && tid == 0) {
-    atomicOr(a.err, 2u);
-    // copies armed for tiles this CTA will not process still write into its
-    // shared memory: wait for them (bounded) before returning
-    for (int q = 0; q < kDctBulkStages; q++) {
-      const int k = it + q, ti = blockIdx.x + k * G;
-      if (ti < a.total_tiles) mbar_wait_bounded(bar0 + 8u * (k % kDctBulkStages), (uint32_t)(k / kDctBulkStages) & 1u);
-    }
-  }
-}
-
-template <int KQ>
-static cudaError_t launch_dct_bulk_t(const DctArgs &a, cudaStream_t s) {
-  const size_t smem = dct_bulk_smem(KQ);
-  int per_sm = 1, sms = 148;
-  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(dct_bulk_kernel<KQ>), 256, smem, &per_sm, &sms);
-  if (e != cudaSuccess) return e;
-  long long grid = (long long)sms * per_sm;
-  if (grid > a.total_tiles) grid = a.total_tiles;
-  dct_bulk_kernel<KQ><<<(unsigned)grid, 256, smem, s>>>(a);
-  return cudaGetLastError();
-}
-
 template <int KQ>
 static cudaError_t launch_dct_fold_t(const DctArgs &a, cudaStream_t s) {
   const size_t smem = sizeof(float) * ((size_t)4 * KQ * 64 + (size_t)kDctTile * dct_row_stride(128));
@@ -1829,18 +1667,6 @@ cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
   // 4 coefficient groups x KQ accumulators cover min(n_mfcc, 32) coefficients per pass
   const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
-  if (a.n_mfcc <= kDctKC && a.n_mels == 128 && a.err) {  // rows by bulk copy (needs the error word)
-    switch ((a.n_mfcc + 3) / 4) {
-      case 1: return launch_dct_bulk_t<1>(a, s);
-      case 2: return launch_dct_bulk_t<2>(a, s);
-      case 3: return launch_dct_bulk_t<3>(a, s);
-      case 4: return launch_dct_bulk_t<4>(a, s);
-      case 5: return launch_dct_bulk_t<5>(a, s);
-      case 6: return launch_dct_bulk_t<6>(a, s);
-      case 7: return launch_dct_bulk_t<7>(a, s);
-      default: return launch_dct_bulk_t<8>(a, s);
-    }
-  }
   if (a.n_mfcc <= kDctKC && a.n_mels == 128) {
     switch ((a.n_mfcc + 3) / 4) {  // ceil(ceil(n_mfcc / 2) / 2)
       case 1: return launch_dct_fold_t<1>(a, s);

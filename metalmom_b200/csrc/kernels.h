@@ -109,7 +109,6 @@ struct DctArgs {
   int n_mels, n_mfcc;
   float top_db;  // <= 0: no floor
   float *out;    // per clip [n_mfcc][n_frames] at clips[c].out_off
-  unsigned *err = nullptr;  // set when a bounded wait runs out (null: kernels without waits only)
 };
 
 constexpr int kDctTile = 64;  // frames per DCT tile (also the onset kernel's tile)

@@ -122,13 +122,11 @@ const DevTables *get_tables(const Group &g, int *status) {
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e == cudaSuccess) {
     e = build_tables(*t, g.sr, g.n_fft, g.win, n_mels, g.fmin, g.fmax, n_mfcc, g.window_zero, s);
-    // the error word of the group's kernels with bounded waits (tensor-core
-    // DFT, bulk-copy DCT)
-    if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
     if (e == cudaSuccess && g.dft_form != DFT_FFT_F32) {
       t->dft = dft_shape(g.n_fft, g.win);
       e = cudaMalloc(&t->dft_basis, dft_basis_bytes(t->dft));
+      if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
+      if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
       if (e == cudaSuccess) e = build_dft_basis(t->dft_basis, t->dft, g.win, g.window_zero, s);
     }
     cudaError_t e2 = cudaStreamSynchronize(s);
@@ -335,7 +333,6 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
     d.n_mfcc = g.n_mfcc_eff;
     d.top_db = g.top_db;
     d.out = b.out;
-    d.err = t->dft_err;
     if ((e = launch_dct(d, s)) != cudaSuccess) return e;
     launches++;
   }

@@ -10,8 +10,9 @@ MetalMom checkout is absent.  The mel filterbank goldens are stored sparsely
 (row, column, value of each nonzero) to keep the archive small; the loader in
 ``tests/goldens.py`` restores them densely.
 
-Usage (needs a MetalMom checkout):
-    python tests/golden/make_golden.py /root/reference
+Usage (needs a MetalMom checkout, given as the argument or in
+MM_REFERENCE_DIR):
+    python tests/golden/make_golden.py /path/to/MetalMom
 """
 
 import os
@@ -64,4 +65,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MM_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_golden.py <MetalMom checkout> (or set MM_REFERENCE_DIR)")
+    main(ref)

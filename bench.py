@@ -503,9 +503,10 @@ def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
 
 def precision_leg(stream, n_clips=512, steps=10):
     """The speech front end (16 kHz, n_fft 512, win 400, hop 160, 80 mels
-    20-8000 Hz, 13 MFCC) on 512 clips x 10 s in three DFT forms: the float32
+    20-8000 Hz, 13 MFCC) on 512 clips x 10 s in four DFT forms: the float32
     FFT, the DFT as a tcgen05 GEMM with bf16x3 split products (float32
-    accumulation) and with plain bf16; device-resident throughput of each
+    accumulation), with plain bf16, and with fp16x3 split products of each
+    frame scaled by a power of two; device-resident throughput of each
     (graph replays, CUDA events) and max/mean mel-dB and MFCC error against the
     FP64 oracle on 4 clips."""
     import torch
@@ -525,7 +526,7 @@ def precision_leg(stream, n_clips=512, steps=10):
     out = {"workload": f"{n_clips} clips x 10 s @16 kHz speech-like, n_fft 512, win 400, hop 160, 80 mels, 13 MFCC",
            "forms": {}}
     hours = n_clips * L / 16000 / 3600.0
-    for form in ("fft", "bf16x3", "bf16"):
+    for form in ("fft", "bf16x3", "bf16", "f16x3"):
         with M.Plan([L] * n_clips, dft=form, **SERVE_SPEECH) as plan:
             res = plan.execute_host(clips, stream=sh)
             for _ in range(3):

@@ -180,11 +180,14 @@ MM_API int32_t mm_amplitude_to_db_device(const float* d_in, int64_t count, float
 
 /* How the spectrum is computed: the float32 FFT (default), or the DFT as a
  * GEMM on the tensor cores (n_fft 256..1024, window <= n_fft) with bf16
- * operands split in two parts (three products, float32 accumulation) or
- * plain bf16.  The GEMM forms exist for the precision comparison. */
+ * operands split in two parts (three products, float32 accumulation), plain
+ * bf16, or fp16 operands split in two parts (three products) after scaling
+ * each frame by a power of two.  The GEMM forms exist for the precision
+ * comparison. */
 #define MM_DFT_FFT_F32 0
 #define MM_DFT_GEMM_BF16X3 1
 #define MM_DFT_GEMM_BF16 2
+#define MM_DFT_GEMM_F16X3 3
 
 /* One front-end parameter group.  Sentinels as in mm_mfcc. */
 typedef struct {
@@ -199,7 +202,7 @@ typedef struct {
     float f_min;
     float f_max;        /* <= 0: sr/2 */
     float top_db;       /* <= 0: no floor; mm_mfcc uses 80 */
-    int32_t dft_form;   /* MM_DFT_FFT_F32 (0), MM_DFT_GEMM_BF16X3 or MM_DFT_GEMM_BF16 */
+    int32_t dft_form;   /* MM_DFT_FFT_F32 (0), MM_DFT_GEMM_BF16X3, MM_DFT_GEMM_BF16 or MM_DFT_GEMM_F16X3 */
 } MMFrontEndParams;
 
 /* MFCC of n_clips clips of any lengths in one batched launch sequence.

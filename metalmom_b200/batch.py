@@ -29,7 +29,7 @@ def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, cent
     p.f_max = float(fmax) if fmax is not None else 0.0
     p.top_db = float(top_db) if top_db is not None else 0.0
     p.dft_form = {"fft": lib.MM_DFT_FFT_F32, "bf16x3": lib.MM_DFT_GEMM_BF16X3,
-                  "bf16": lib.MM_DFT_GEMM_BF16}[dft]
+                  "bf16": lib.MM_DFT_GEMM_BF16, "f16x3": lib.MM_DFT_GEMM_F16X3}[dft]
     return p
 
 

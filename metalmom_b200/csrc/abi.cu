@@ -485,7 +485,7 @@ int mm::resolve_frontend(const MMFrontEndParams *p, Group &g) {
   if (p->n_mfcc < 0 || (p->pad_mode != MM_PAD_CONSTANT && p->pad_mode != MM_PAD_REFLECT))
     return MM_ERR_INVALID_INPUT;
   if (!is_pow2(p->n_fft) || !supported_size(g)) return MM_ERR_INVALID_INPUT;
-  if (p->dft_form < MM_DFT_FFT_F32 || p->dft_form > MM_DFT_GEMM_BF16) return MM_ERR_INVALID_INPUT;
+  if (p->dft_form < MM_DFT_FFT_F32 || p->dft_form > MM_DFT_GEMM_F16X3) return MM_ERR_INVALID_INPUT;
   if (p->dft_form != MM_DFT_FFT_F32 && !dft_supported(g.n_fft, g.win)) return MM_ERR_INVALID_INPUT;
   g.dft_form = p->dft_form;
   g.mode = MODE_MELDB;

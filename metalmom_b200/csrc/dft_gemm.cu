@@ -36,6 +36,7 @@
 // Every wait is bounded: a wait that runs out sets the error word and the
 // CTA stops, releases its tensor memory and returns.
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <math.h>
 #include <stdint.h>
 
@@ -94,9 +95,22 @@ __host__ __device__ __forceinline__ uint32_t sw128(int r, int k) {
   return (uint32_t)r * 128u + ((uint32_t)(((k >> 3) ^ (r & 7))) << 4) + (uint32_t)(k & 7) * 2u;
 }
 
+// Two 16-bit parts of a float64 value: v ~ hi + lo (bf16 or fp16).
+__device__ __forceinline__ void split_parts(double v, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+  hi = __double2bfloat16(v);
+  lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+}
+__device__ __forceinline__ void split_parts(double v, __half &hi, __half &lo) {
+  hi = __double2half(v);
+  lo = __double2half(v - (double)__half2float(hi));
+}
+
 // B image: [tile][chunk][part hi/lo][tile_cols rows x 128 bytes], values in
-// float64 (window and twiddle), split into bf16 hi + lo.
-__global__ void build_dft_basis_kernel(__nv_bfloat16 *img, DftShape s, int win, int window_zero) {
+// float64 (window and twiddle), split into two 16-bit parts (T: bf16 or fp16;
+// the fp16 parts of values up to 1 lose nothing to range: lo parts below
+// fp16's normal range keep an absolute precision of 2^-24).
+template <typename T>
+__global__ void build_dft_basis_kernel(T *img, DftShape s, int win, int window_zero) {
   const long long total = (long long)s.ntiles * s.kchunks * s.tile_cols * kDftKC;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= total) return;
@@ -122,12 +136,12 @@ __global__ void build_dft_basis_kernel(__nv_bfloat16 *img, DftShape s, int win, 
       v = part == 0 ? w * cs : -w * sn;
     }
   }
-  const __nv_bfloat16 hi = __double2bfloat16(v);
-  const __nv_bfloat16 lo = __double2bfloat16(v - (double)__bfloat162float(hi));
+  T hi, lo;
+  split_parts(v, hi, lo);
   const size_t tile_bytes = (size_t)s.tile_cols * 128;
   char *base = reinterpret_cast<char *>(img) + ((size_t)(nt * s.kchunks + kc) * 2) * tile_bytes;
-  *reinterpret_cast<__nv_bfloat16 *>(base + sw128(r, j)) = hi;
-  *reinterpret_cast<__nv_bfloat16 *>(base + tile_bytes + sw128(r, j)) = lo;
+  *reinterpret_cast<T *>(base + sw128(r, j)) = hi;
+  *reinterpret_cast<T *>(base + tile_bytes + sw128(r, j)) = lo;
 }
 
 // ---------------------------------------------------------------------------
@@ -144,10 +158,13 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
   return d;
 }
 
-// kind::f16 instruction descriptor: f32 accumulator, bf16 A and B, both
-// K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kDftM >> 4) << 24);
+// kind::f16 instruction descriptor: f32 accumulator, A and B both bf16
+// (F16 false) or both fp16 (F16 true; one instruction never mixes the two),
+// both K-major, M = 128, N = n.
+template <bool F16>
+__host__ __device__ constexpr uint32_t idesc_f16kind(int n) {
+  return (1u << 4) | (F16 ? 0u : (1u << 7) | (1u << 10)) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(kDftM >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
@@ -179,16 +196,26 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
 }
 
-// Two bf16 parts of 8 floats, packed for one 16-byte store each.
+// Two 16-bit parts (bf16, or fp16 when F16) of 8 floats, packed for one
+// 16-byte store each.
+template <bool F16>
 __device__ __forceinline__ void split8(const float *x, uint4 &hi, uint4 &lo) {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int i = 0; i < 4; i++) {
-    const __nv_bfloat162 a = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
-    const float2 af = __bfloat1622float2(a);
-    const __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * i] - af.x, x[2 * i + 1] - af.y);
-    h[i] = *reinterpret_cast<const uint32_t *>(&a);
-    l[i] = *reinterpret_cast<const uint32_t *>(&b);
+    if constexpr (F16) {
+      const __half2 a = __floats2half2_rn(x[2 * i], x[2 * i + 1]);
+      const float2 af = __half22float2(a);
+      const __half2 b = __floats2half2_rn(x[2 * i] - af.x, x[2 * i + 1] - af.y);
+      h[i] = *reinterpret_cast<const uint32_t *>(&a);
+      l[i] = *reinterpret_cast<const uint32_t *>(&b);
+    } else {
+      const __nv_bfloat162 a = __floats2bfloat162_rn(x[2 * i], x[2 * i + 1]);
+      const float2 af = __bfloat1622float2(a);
+      const __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * i] - af.x, x[2 * i + 1] - af.y);
+      h[i] = *reinterpret_cast<const uint32_t *>(&a);
+      l[i] = *reinterpret_cast<const uint32_t *>(&b);
+    }
   }
   hi = make_uint4(h[0], h[1], h[2], h[3]);
   lo = make_uint4(l[0], l[1], l[2], l[3]);
@@ -248,8 +275,11 @@ __host__ __device__ inline DftSmem dft_smem_layout(const DftShape &s, int n_mels
   return L;
 }
 
-template <int SPLIT>
-__global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, DftShape S, const __nv_bfloat16 *basis,
+// F16: fp16 parts, with each frame's samples scaled by a.frame_scale (a power
+// of two, so that the frame's largest sample is in [0.5, 1)) before the
+// split and |X|^2 scaled back exactly in the epilogue.
+template <int SPLIT, bool F16>
+__global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, DftShape S, const void *basis,
                                                                    unsigned *err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -315,6 +345,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
       const bool valid = t < cd.n_frames;
       const float *sig = a.signal + cd.sig_off;
       const long long s0 = (long long)t * a.hop - a.pad + S.k0 + kDftRowCols * part;
+      const float sc = (F16 && valid) ? __ldg(a.frame_scale + cd.frame_off + t) : 1.0f;
       // samples two chunks ahead (a chunk's samples serve every N tile)
       const int nchunks = S.ntiles * S.kchunks;
       float xn[kDftRowCols], xn2[kDftRowCols];
@@ -332,7 +363,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
               break;
             }
             unsigned char *bs = sm + Ly.b0 + (size_t)sb * Ly.b_stage;
-            const char *src = reinterpret_cast<const char *>(basis) + (size_t)(nt * S.kchunks + kc) * 2 * b_img;
+            const char *src = static_cast<const char *>(basis) + (size_t)(nt * S.kchunks + kc) * 2 * b_img;
             mbar_expect_tx(b_full(sb), SPLIT == 3 ? 2u * b_img : b_img);
             bulk_g2s(smem_u32(bs), src, b_img, b_full(sb));
             if (SPLIT == 3) bulk_g2s(smem_u32(bs + Ly.b_img), src + b_img, b_img, b_full(sb));
@@ -356,7 +387,14 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
 #pragma unroll
           for (int q = 0; q < kDftRowCols / 8; q++) {
             uint4 hi, lo;
-            split8(x + 8 * q, hi, lo);
+            if constexpr (F16) {
+              float xs[8];
+#pragma unroll
+              for (int u = 0; u < 8; u++) xs[u] = x[8 * q + u] * sc;
+              split8<true>(xs, hi, lo);
+            } else {
+              split8<false>(x + 8 * q, hi, lo);
+            }
             const uint32_t off = sw128(row, kDftRowCols * part + 8 * q);
             *reinterpret_cast<uint4 *>(as + off) = hi;
             if (SPLIT == 3) *reinterpret_cast<uint4 *>(as + kDftM * 128 + off) = lo;
@@ -374,7 +412,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   } else if (warp == kDftMmaWarp) {
     // ---------------- MMA issue (one thread)
     if (lane == 0) {
-      const uint32_t idesc = idesc_bf16(S.tile_cols);
+      const uint32_t idesc = idesc_f16kind<F16>(S.tile_cols);
       uint32_t c = 0, j = 0;  // chunk and accumulator-tile counters
       bool ok = true;
       for (int tile = t_begin; tile < t_end && ok; tile++) {
@@ -440,9 +478,15 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
       const int t = (tile - cd.tile_base) * kDftM + row;
       const bool valid = t < cd.n_frames;
       float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
+      float isc2 = 1.0f;  // F16: 1 / scale^2, a power of two (exact)
+      if constexpr (F16) {
+        const float sc = valid ? __ldg(a.frame_scale + cd.frame_off + t) : 1.0f;
+        isc2 = 1.0f / (sc * sc);
+      }
       int cur = 0;
       float Rprev = 0.0f, Rcur = 0.0f, Fcur = 0.0f, chk = 0.0f, fmax_ = -INFINITY;
       auto emit = [&](int m, float v) {
+        if constexpr (F16) v *= isc2;
         if (seg_s[m].y) v = __int_as_float(0x7fc00000);
         const float val = db10_frame(v, a.amin, ref_db);
         if (valid) dst[m] = val;
@@ -508,30 +552,96 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kDftTmemCols) : "memory");
 }
 
-cudaError_t build_dft_basis(__nv_bfloat16 *img, const DftShape &s, int win, int window_zero, cudaStream_t st) {
+cudaError_t build_dft_basis(void *img, const DftShape &s, int win, int window_zero, bool f16, cudaStream_t st) {
   const long long total = (long long)s.ntiles * s.kchunks * s.tile_cols * kDftKC;
-  build_dft_basis_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(img, s, win, window_zero);
+  const unsigned blocks = (unsigned)((total + 255) / 256);
+  if (f16)
+    build_dft_basis_kernel<__half><<<blocks, 256, 0, st>>>(static_cast<__half *>(img), s, win, window_zero);
+  else
+    build_dft_basis_kernel<__nv_bfloat16><<<blocks, 256, 0, st>>>(static_cast<__nv_bfloat16 *>(img), s, win,
+                                                                   window_zero);
   return cudaGetLastError();
 }
 
-cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, const __nv_bfloat16 *basis,
+// Per frame: 2^-e with 2^(e-1) <= max |x| < 2^e over the samples the frame's
+// DFT reads (the window's support, s.k0 .. s.k0 + s.kw), so the scaled
+// samples lie in (-1, 1) and their fp16 lo parts keep 2^-24 of the frame's
+// largest sample even where they fall below fp16's normal range.  Frames that
+// reach into the padding take the maximum over a range that covers every
+// sample the padding rule (zeros or a mirror) can read.  A frame of zeros, or
+// one holding a non-finite sample, gets 1 (the non-finite value then reaches
+// the spectrum, as in the FFT form).  e is clamped to [-63, 63] so that the
+// epilogue's 1 / scale^2 is a normal float.  One warp per frame.
+__global__ void frame_scale_kernel(FrontArgs a, DftShape s, float *scale) {
+  const int lane = threadIdx.x & 31;
+  const int warps = (blockDim.x >> 5) * gridDim.x;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  for (long long w = w0; w < (long long)a.total_tiles * kDftM; w += warps) {
+    const int tile = (int)(w / kDftM), row = (int)(w - (long long)tile * kDftM);
+    const int cl = __ldg(a.tile_clip + tile);
+    const ClipDesc cd = load_clip(a.clips + cl);
+    const int t = (tile - cd.tile_base) * kDftM + row;
+    if (t >= cd.n_frames) continue;  // warp-uniform
+    const float *sig = a.signal + cd.sig_off;
+    long long lo = (long long)t * a.hop - a.pad + s.k0, hi = lo + s.kw;
+    if (lo < 0 || hi > cd.length) {  // mirrored samples lie within kw of the edge they mirror
+      lo = lo - s.kw;
+      hi = hi + s.kw;
+    }
+    lo = lo < 0 ? 0 : lo;
+    hi = hi > cd.length ? cd.length : hi;
+    float m = 0.0f;
+    bool bad = false;
+    for (long long i = lo + lane; i < hi; i += 32) {
+      const float v = __ldg(sig + i);
+      bad |= !isfinite(v);
+      m = fmaxf(m, fabsf(v));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) {
+      float sc = 1.0f;
+      if (!bad && m > 0.0f) {
+        int e = ilogbf(m) + 1;  // 2^(e-1) <= m < 2^e
+        e = e < -63 ? -63 : (e > 63 ? 63 : e);
+        sc = ldexpf(1.0f, -e);
+      }
+      scale[cd.frame_off + t] = sc;
+    }
+  }
+}
+
+cudaError_t launch_frame_scale(const FrontArgs &a, const DftShape &s, cudaStream_t st) {
+  if (a.total_tiles <= 0 || !a.frame_scale) return cudaSuccess;
+  const long long warps = (long long)a.total_tiles * kDftM;
+  const long long blocks = std::min<long long>((warps + 7) / 8, 148LL * 16);
+  frame_scale_kernel<<<(unsigned)blocks, 256, 0, st>>>(a, s, const_cast<float *>(a.frame_scale));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, const void *basis,
                             unsigned *err, cudaStream_t st, int *launched) {
   if (launched) *launched = 0;
   if (a.total_tiles <= 0) return cudaSuccess;
   if (!a.mel_seg_ok) return cudaErrorInvalidValue;  // the epilogue needs the per-bin split
   if (s.tile_cols > 256) return cudaErrorInvalidValue;
+  if (form == DFT_GEMM_F16X3 && !a.frame_scale) return cudaErrorInvalidValue;
   const size_t smem = dft_smem_layout(s, a.n_mels).total;
-  const void *kern = form == DFT_GEMM_BF16X3 ? reinterpret_cast<const void *>(dft_gemm_kernel<3>)
-                                              : reinterpret_cast<const void *>(dft_gemm_kernel<1>);
+  const void *kern = form == DFT_GEMM_BF16X3   ? reinterpret_cast<const void *>(dft_gemm_kernel<3, false>)
+                     : form == DFT_GEMM_F16X3 ? reinterpret_cast<const void *>(dft_gemm_kernel<3, true>)
+                                              : reinterpret_cast<const void *>(dft_gemm_kernel<1, false>);
   int per_sm = 1, sms = 148;
   cudaError_t e = persistent_geometry(kern, kDftThreads, smem, &per_sm, &sms);
   if (e != cudaSuccess) return e;
   long long grid = sms;  // one CTA per SM: it holds all 512 TMEM columns
   if (grid > a.total_tiles) grid = a.total_tiles;
   if (form == DFT_GEMM_BF16X3)
-    dft_gemm_kernel<3><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);
+    dft_gemm_kernel<3, false><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);
+  else if (form == DFT_GEMM_F16X3)
+    dft_gemm_kernel<3, true><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);
   else
-    dft_gemm_kernel<1><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);
+    dft_gemm_kernel<1, false><<<(unsigned)grid, kDftThreads, smem, st>>>(a, s, basis, err);
   if (launched) *launched = (int)grid;
   return cudaGetLastError();
 }

@@ -30,7 +30,7 @@ __host__ __device__ constexpr bool mode_has_mel(int mode) { return mode == MODE_
 enum PadMode : int { PAD_CONSTANT = 0, PAD_REFLECT = 1 };
 
 // How the spectrum is computed (MMFrontEndParams.dft_form).
-enum DftForm : int { DFT_FFT_F32 = 0, DFT_GEMM_BF16X3 = 1, DFT_GEMM_BF16 = 2 };
+enum DftForm : int { DFT_FFT_F32 = 0, DFT_GEMM_BF16X3 = 1, DFT_GEMM_BF16 = 2, DFT_GEMM_F16X3 = 3 };
 
 // Geometry of the DFT-as-GEMM form: bins, N tiles of tile_cols columns
 // (cos / -sin per bin), the window support [k0, k0 + kw) cut into K chunks.
@@ -63,9 +63,10 @@ struct DevTables {
   int2 *mel_lane = nullptr;    // per lane {flush mask, first slot | chain length | zero slot}
   int *mel_band = nullptr;     // per band: head slot of m | head slot of m+1 | NaN flag
   int mel_lane_ok = 0;
-  // DFT-as-GEMM form only: the windowed DFT basis as bf16 hi/lo images and an
-  // error word the kernel sets when a bounded wait runs out.
-  __nv_bfloat16 *dft_basis = nullptr;
+  // DFT-as-GEMM form only: the windowed DFT basis as hi/lo images (bf16, or
+  // fp16 for DFT_GEMM_F16X3) and an error word the kernel sets when a bounded
+  // wait runs out.
+  void *dft_basis = nullptr;
   DftShape dft{};
   unsigned *dft_err = nullptr;
   float *dct = nullptr;        // [n_mfcc_eff][n_mels] DCT-II ortho basis
@@ -96,6 +97,9 @@ struct FrontArgs {
   float amin, ref;
   float *out;
   unsigned *clip_max;  // MODE_MELDB: order-preserving encoded max per clip
+  // DFT_GEMM_F16X3 only: per frame (frame-major, as the log-mel rows) the
+  // power of two the frame's samples are scaled by before the fp16 split
+  float *frame_scale = nullptr;
 };
 
 struct DctArgs {
@@ -186,9 +190,12 @@ constexpr int kDftVariant = 4;  // launch "variant" of such groups (128-frame ti
 bool dft_supported(int n_fft, int win);
 DftShape dft_shape(int n_fft, int win);
 size_t dft_basis_bytes(const DftShape &s);
-cudaError_t build_dft_basis(__nv_bfloat16 *img, const DftShape &s, int win, int window_zero, cudaStream_t st);
-cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, const __nv_bfloat16 *basis,
+cudaError_t build_dft_basis(void *img, const DftShape &s, int win, int window_zero, bool f16, cudaStream_t st);
+cudaError_t launch_dft_gemm(int form, const FrontArgs &a, const DftShape &s, const void *basis,
                             unsigned *err, cudaStream_t st, int *launched);
+// DFT_GEMM_F16X3: the per-frame scale of every frame of the batch into
+// a.frame_scale (one warp per frame over the window's support).
+cudaError_t launch_frame_scale(const FrontArgs &a, const DftShape &s, cudaStream_t st);
 
 // Frame kernel: framing + window + rFFT + |X|^2 + mode epilogue.
 cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a, int grid_limit,

@@ -110,7 +110,9 @@ const DevTables *get_tables(const Group &g, int *status) {
   }
   const int n_mels = mode_has_mel(g.mode) ? g.n_mels : 0;
   const int n_mfcc = (g.mode == MODE_MELDB) ? g.n_mfcc_eff : 0;
-  TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax, g.dft_form != 0 ? 1 : 0};
+  // basis images: none (FFT), bf16 (the two bf16 forms) or fp16 (the fp16-split form)
+  const int basis_kind = g.dft_form == DFT_GEMM_F16X3 ? 2 : (g.dft_form != DFT_FFT_F32 ? 1 : 0);
+  TableKey k{dev, g.sr, g.n_fft, g.win, g.window_zero, n_mels, n_mfcc, g.fmin, g.fmax, basis_kind};
   std::lock_guard<std::mutex> lock(g_table_mu);
   auto it = g_tables.find(k);
   if (it != g_tables.end()) {
@@ -127,7 +129,8 @@ const DevTables *get_tables(const Group &g, int *status) {
       e = cudaMalloc(&t->dft_basis, dft_basis_bytes(t->dft));
       if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
       if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
-      if (e == cudaSuccess) e = build_dft_basis(t->dft_basis, t->dft, g.win, g.window_zero, s);
+      if (e == cudaSuccess)
+        e = build_dft_basis(t->dft_basis, t->dft, g.win, g.window_zero, g.dft_form == DFT_GEMM_F16X3, s);
     }
     cudaError_t e2 = cudaStreamSynchronize(s);
     if (e == cudaSuccess) e = e2;
@@ -197,11 +200,12 @@ void make_layout(const Group &g, const int64_t *lengths, int n, Layout &L) {
   L.total_frames = frames;
   L.out_elems = out;
   L.meldb_elems = (g.mode == MODE_MELDB) ? frames * (long long)g.n_mels : 0;
+  L.scale_elems = (g.mode == MODE_MELDB && g.dft_form == DFT_GEMM_F16X3) ? frames : 0;
 }
 
 namespace {
 struct Offsets {
-  size_t signal, clips, tile_clip, dct_clip, dct_first, desc_end, clip_max, meldb, out, total;
+  size_t signal, clips, tile_clip, dct_clip, dct_first, desc_end, clip_max, meldb, out, scale, total;
 };
 Offsets offsets(const Layout &L) {
   Offsets o;
@@ -225,6 +229,8 @@ Offsets offsets(const Layout &L) {
   p = round_up(p + sizeof(float) * (size_t)L.meldb_elems, 256);
   o.out = p;
   p = round_up(p + sizeof(float) * (size_t)L.out_elems, 256);
+  o.scale = p;
+  p = round_up(p + sizeof(float) * (size_t)L.scale_elems, 256);
   o.total = p;
   return o;
 }
@@ -242,6 +248,7 @@ size_t carve_arena(const Group &, const Layout &L, char *base, DevBatch &b) {
   b.clip_max = reinterpret_cast<unsigned *>(base + o.clip_max);
   b.meldb = reinterpret_cast<float *>(base + o.meldb);
   b.out = reinterpret_cast<float *>(base + o.out);
+  b.frame_scale = L.scale_elems > 0 ? reinterpret_cast<float *>(base + o.scale) : nullptr;
   return o.desc_end - o.clips;
 }
 
@@ -297,6 +304,11 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.out = (g.mode == MODE_MELDB) ? b.meldb : b.out;
   a.clip_max = b.clip_max;
   int grid = 0;
+  if (g.dft_form == DFT_GEMM_F16X3 && g.mode == MODE_MELDB) {
+    a.frame_scale = b.frame_scale;
+    if ((e = launch_frame_scale(a, t->dft, s)) != cudaSuccess) return e;
+    launches++;
+  }
   if (g.dft_form != DFT_FFT_F32 && g.mode == MODE_MELDB)
     e = launch_dft_gemm(g.dft_form, a, t->dft, t->dft_basis, t->dft_err, s, &grid);
   else

@@ -60,6 +60,7 @@ struct Layout {
   std::vector<int> dct_tile_clip;   // DCT tiles
   std::vector<int> dct_tile_first;
   long long sig_elems = 0, total_frames = 0, out_elems = 0, meldb_elems = 0;
+  long long scale_elems = 0;  // per-frame scales (fp16-split DFT form only)
   int F = 1;
 };
 void make_layout(const Group &g, const int64_t *lengths, int n, Layout &L);
@@ -74,6 +75,7 @@ struct DevBatch {
   unsigned *clip_max = nullptr;
   float *meldb = nullptr;
   float *out = nullptr;
+  float *frame_scale = nullptr;
 };
 
 // Bytes of one device arena holding a whole batch (signal included).

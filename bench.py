@@ -698,9 +698,9 @@ def run_ours(args, rank, world, local_rank):
         flops_fft = 2.5 * N_FFT * np.log2(N_FFT) * T_total
         traffic = None
         warp = tune["best"] == 3
-        kname = "frame_warp_kernel<11>" if warp else f"frontend_kernel<11,V{tune['best']},MELDB>"
-        tp = os.path.join(ROOT, "profiles", ("frame_warp_kernel" if warp else "frontend_kernel")
-                          + "_256clips_traffic.txt")
+        kname = {3: "frame_warp_kernel<11>", 5: "frame_tc_kernel"}.get(
+            tune["best"], f"frontend_kernel<11,V{tune['best']},MELDB>")
+        tp = os.path.join(ROOT, "profiles", kname.split("<")[0] + "_256clips_traffic.txt")
         if os.path.exists(tp) and n_clips == N_CLIPS:
             for line in open(tp):
                 if line.startswith("bytes_per_launch:"):

@@ -267,10 +267,12 @@ MM_API int32_t mm_plan_execute_host(mm_plan plan, const float* const* signals, f
 /* Autotuning of the frame kernel's launch variant, process-wide per n_fft:
  * variants 0-2 are the CTA-per-tile kernel with different frames per CTA and
  * register budgets; variant 3 (MFCC path, n_fft 256..2048) is the
- * warp-per-frame kernel.  mm_autotune times every variant
- * on n_clips synthetic clips of clip_samples samples (reps launches each),
- * writes the per-variant milliseconds to variant_ms (up to 4 entries), keeps
- * the fastest and returns it in *best_variant.  Plans and calls made
+ * warp-per-frame kernel (warp pair at 4096); variant 5 (MFCC path, n_fft 2048)
+ * is the tensor-core kernel (both 32-point DFT stages as fp16x3 tcgen05
+ * GEMMs).  mm_autotune times every variant that applies on n_clips synthetic
+ * clips of clip_samples samples (reps launches each), writes each variant's
+ * milliseconds to variant_ms[variant] (6 entries; 0 for variants not timed),
+ * keeps the fastest and returns it in *best_variant.  Plans and calls made
  * afterwards use the tuned variant. */
 MM_API int32_t mm_autotune(mm_context ctx, const MMFrontEndParams* params, int64_t clip_samples,
                            int32_t n_clips, int32_t reps, float* variant_ms, int32_t* best_variant);

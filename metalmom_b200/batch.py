@@ -36,9 +36,9 @@ def frontend_params(sr=22050, n_fft=2048, hop_length=None, win_length=None, cent
 def autotune(clip_samples=661500, n_clips=32, reps=10, **params):
     """Time every launch variant of the frame kernel for these parameters on
     synthetic clips, keep the fastest for this n_fft (process-wide) and return
-    {"best": v, "ms": [per-variant ms]}."""
+    {"best": v, "ms": {variant: ms}}."""
     p = frontend_params(**params)
-    ms = ffi.new("float[4]")
+    ms = ffi.new("float[6]")
     best = ffi.new("int32_t*")
     ctx = lib.mm_init()
     try:
@@ -47,8 +47,7 @@ def autotune(clip_samples=661500, n_clips=32, reps=10, **params):
             raise RuntimeError(f"mm_autotune failed with status {st}")
     finally:
         lib.mm_destroy(ctx)
-    n = sum(1 for i in range(4) if ms[i] > 0)
-    return {"best": int(best[0]), "ms": [float(ms[i]) for i in range(n)]}
+    return {"best": int(best[0]), "ms": {i: float(ms[i]) for i in range(6) if ms[i] > 0}}
 
 
 def tune_set(n_fft, variant):

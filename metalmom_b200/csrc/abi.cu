@@ -85,7 +85,8 @@ int run_batch(const Group &g_in, const float *const *signals, const int64_t *len
   if ((e = cudaMemcpyAsync(h, b.out, out_bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_status(e);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e);
-  if (t->dft_err) {  // a bounded wait of the tensor-core kernel ran out
+  if (t->dft_err && (g.dft_form != DFT_FFT_F32 || g.variant == kTcVariant)) {
+    // a bounded wait of a tensor-core kernel ran out
     unsigned flag = 0;
     if ((e = cudaMemcpy(&flag, t->dft_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess)
       return cuda_status(e);
@@ -519,7 +520,9 @@ int32_t mm_mfcc_batch(mm_context ctx, const float *const *signals, const int64_t
 }
 
 int32_t mm_tune_set(int32_t n_fft, int32_t variant) {
-  if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 || variant > kWarpVariant) return MM_ERR_INVALID_INPUT;
+  if (!is_pow2(n_fft) || ilog2(n_fft) > 15 || variant < 0 ||
+      (variant > kWarpVariant && !(variant == kTcVariant && n_fft == 2048)))
+    return MM_ERR_INVALID_INPUT;
   set_tuned_variant(ilog2(n_fft), variant);
   return MM_OK;
 }
@@ -539,6 +542,10 @@ int32_t mm_autotune(mm_context ctx, const MMFrontEndParams *params, int64_t clip
   const DevTables *t = get_tables(g, &st);
   if (!t) return st;
   const int nv = frame_variants(g.log2n, g.mode, 1);
+  // candidates: the frame variants, and the tensor-core kernel where it applies
+  std::vector<int> cand;
+  for (int v = 0; v < nv; v++) cand.push_back(v);
+  if (g.log2n == 11 && g.mode == MODE_MELDB && g.dft_form == DFT_FFT_F32) cand.push_back(kTcVariant);
   std::vector<int64_t> lengths(n_clips, clip_samples);
   cudaStream_t s = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -547,7 +554,8 @@ int32_t mm_autotune(mm_context ctx, const MMFrontEndParams *params, int64_t clip
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
   float best_ms = 0.0f;
   int best = 0;
-  for (int v = 0; v < nv && e == cudaSuccess; v++) {
+  for (size_t ci = 0; ci < cand.size() && e == cudaSuccess; ci++) {
+    const int v = cand[ci];
     Group gv = g;
     gv.variant = v;
     Layout L;
@@ -571,7 +579,7 @@ int32_t mm_autotune(mm_context ctx, const MMFrontEndParams *params, int64_t clip
     cudaFree(arena);
     ms /= reps;
     if (variant_ms) variant_ms[v] = ms;
-    if (e == cudaSuccess && (v == 0 || ms < best_ms)) {
+    if (e == cudaSuccess && (ci == 0 || ms < best_ms)) {
       best_ms = ms;
       best = v;
     }

@@ -43,6 +43,7 @@
 #include <algorithm>
 
 #include "async_copy.cuh"
+#include "tcgen05.cuh"
 #include "frame_common.cuh"
 #include "kernels.h"
 
@@ -87,12 +88,6 @@ bool dft_supported(int n_fft, int win) { return n_fft >= 256 && n_fft <= 1024 &&
 
 size_t dft_basis_bytes(const DftShape &s) {
   return (size_t)s.ntiles * s.kchunks * 2 * (size_t)s.tile_cols * 128;
-}
-
-// Byte offset of element (row r, k) in a K-major tile with 128-byte rows and
-// the 128-byte swizzle (16-byte chunk index XOR row % 8).
-__host__ __device__ __forceinline__ uint32_t sw128(int r, int k) {
-  return (uint32_t)r * 128u + ((uint32_t)(((k >> 3) ^ (r & 7))) << 4) + (uint32_t)(k & 7) * 2u;
 }
 
 // Two 16-bit parts of a float64 value: v ~ hi + lo (bf16 or fp16).
@@ -147,55 +142,6 @@ __global__ void build_dft_basis_kernel(T *img, DftShape s, int win, int window_z
 // ---------------------------------------------------------------------------
 // tcgen05 / mbarrier helpers (inline PTX)
 // ---------------------------------------------------------------------------
-// K-major operand, 128-byte swizzle: rows of 128 bytes, 8-row groups 1024
-// bytes apart (stride byte offset), sm_100 descriptor version 1.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
-  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)1u << 16;            // leading byte offset (unused by swizzled K-major)
-  d |= (uint64_t)(1024u >> 4) << 32;  // stride byte offset
-  d |= (uint64_t)1u << 46;            // descriptor version
-  d |= (uint64_t)2u << 61;            // 128-byte swizzle
-  return d;
-}
-
-// kind::f16 instruction descriptor: f32 accumulator, A and B both bf16
-// (F16 false) or both fp16 (F16 true; one instruction never mixes the two),
-// both K-major, M = 128, N = n.
-template <bool F16>
-__host__ __device__ constexpr uint32_t idesc_f16kind(int n) {
-  return (1u << 4) | (F16 ? 0u : (1u << 7) | (1u << 10)) | ((uint32_t)(n >> 3) << 17) |
-         ((uint32_t)(kDftM >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
-  const uint32_t z = 0;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-      "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
-               : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
-
 // Two 16-bit parts (bf16, or fp16 when F16) of 8 floats, packed for one
 // 16-byte store each.
 template <bool F16>
@@ -412,7 +358,7 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
   } else if (warp == kDftMmaWarp) {
     // ---------------- MMA issue (one thread)
     if (lane == 0) {
-      const uint32_t idesc = idesc_f16kind<F16>(S.tile_cols);
+      const uint32_t idesc = idesc_f16kind<F16>(S.tile_cols, kDftM);
       uint32_t c = 0, j = 0;  // chunk and accumulator-tile counters
       bool ok = true;
       for (int tile = t_begin; tile < t_end && ok; tile++) {
@@ -437,10 +383,10 @@ __global__ void __launch_bounds__(kDftThreads, 1) dft_gemm_kernel(FrontArgs a, D
 #pragma unroll
             for (int kk = 0; kk < kDftKC / 16; kk++) {
               const uint64_t dah = desc_sw128(ah + kk * 32), dbh = desc_sw128(bh + kk * 32);
-              umma_bf16(acc, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
+              umma_f16kind(acc, dah, dbh, idesc, (kc > 0 || kk > 0) ? 1u : 0u);
               if (SPLIT == 3) {
-                umma_bf16(acc, dah, desc_sw128(bl + kk * 32), idesc, 1u);
-                umma_bf16(acc, desc_sw128(al + kk * 32), dbh, idesc, 1u);
+                umma_f16kind(acc, dah, desc_sw128(bl + kk * 32), idesc, 1u);
+                umma_f16kind(acc, desc_sw128(al + kk * 32), dbh, idesc, 1u);
               }
             }
             umma_commit(a_empty(sa));  // the stages are free once these MMAs complete

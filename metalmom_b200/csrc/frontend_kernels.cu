@@ -117,6 +117,7 @@ static int frames_for(int v) {
 
 int frames_per_tile(int log2n, int variant) {
   if (variant == kDftVariant) return 128;
+  if (variant == kTcVariant && log2n == 11) return kTcFramesPerTile;
   if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0) return warp_frames_per_tile(log2n);
   switch (log2n) {
     case 5: return frames_for<5>(variant);
@@ -1316,6 +1317,7 @@ cudaError_t launch_frontend(int log2n, int mode, int variant, const FrontArgs &a
     case MODE_COMPLEX: return launch_mode<MODE_COMPLEX, 0>(log2n, variant, a, grid_limit, s, launched);
     case MODE_MELDB:
       if (pw != 0) return cudaErrorInvalidValue;
+      if (variant == kTcVariant && log2n == 11) return launch_frontend_tc(a, grid_limit, s, launched);
       if (variant == kWarpVariant && warp_frames_per_tile(log2n) > 0)
         return launch_frontend_warp(log2n, a, grid_limit, s, launched);
       return launch_mode<MODE_MELDB, 0>(log2n, variant, a, grid_limit, s, launched);

@@ -30,9 +30,13 @@
 #include <algorithm>
 #include <type_traits>
 
+#include <cuda_fp16.h>
+
+#include "async_copy.cuh"
 #include "fft_radix.cuh"
 #include "frame_common.cuh"
 #include "kernels.h"
+#include "tcgen05.cuh"
 
 namespace mm {
 
@@ -880,6 +884,535 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
   if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+}
+
+// ---------------------------------------------------------------------------
+// n_fft 2048 with both 32-point DFT stages on the tensor cores (launch
+// variant 5).  The frame is the packed sequence z[n] (n = n1 + 32 n2) of the
+// warp kernel, 1 024 complex points as 32 x 32:
+//
+//   stage 1  Y[n1][k2] = sum_n2 z[n1 + 32 n2] W_32^(n2 k2)      (GEMM 1)
+//   twiddle  Y[n1][k2] *= W_1024^(n1 k2)                         (CUDA cores)
+//   stage 2  Z[k2 + 32 k1] = sum_n1 Y[n1][k2] W_32^(n1 k1)      (GEMM 2)
+//
+// Both GEMMs take the same B: the 32-point DFT in real form (64 x 64, inputs
+// [re | im], outputs [re | im]), built in float64 and split into fp16 hi +
+// lo parts.  Four frames make one M = 128 tile: GEMM 1's A has a row per
+// (frame, n1) and K = [re z | im z] over n2 (K-major, the lane of a warp
+// holds its row); GEMM 2's A has a row per (frame, k2) and K over n1, and is
+// written MN-major (lane n1 holds K-rows n1 and 32 + n1, each 32 contiguous
+// values along M).  Each GEMM is hi*hi + hi*lo + lo*hi in fp16 with float32
+// accumulation in tensor memory, 12 tcgen05.mma of M 128 x N 64 x K 16,
+// issued by one thread.  fp16 needs the frame in range: the windowed samples
+// are scaled by 2^-e (their largest magnitude into [0.5, 1)), which keeps the
+// split at float32 grade (the lo parts of small values keep 2^-24 of the
+// frame's largest sample), and the band sums are scaled back by 2^(2e),
+// exactly.  GEMM 2's output row (frame, k2) holds Z[k2 + 32 k1] for all k1,
+// the register layout of the warp kernel after its stage 2, so the real
+// split, the filterbank walk, the log and the running clip maximum are the
+// warp kernel's.
+//
+// CTA: 16 warps in 4 independent groups of 4 (one frame per warp, one M = 128
+// tile per group), one CTA per SM holding 256 tensor-memory columns (64 per
+// group).  A group's shared region holds its A images (hi, lo; reused by
+// both GEMMs) and, after GEMM 2 has completed, the four frames' spectra.  Per
+// tile a group synchronises on three named barriers (A1 written, A2 written,
+// spectra read) and two mbarriers the MMA commits arrive on.  Every mbarrier
+// wait is bounded: a wait that runs out sets *a.err, the group leaves the
+// loop together at its next barrier (a barrier reduction), and the CTA waits
+// (bounded) for its MMAs before releasing tensor memory.
+// ---------------------------------------------------------------------------
+struct TcShape {
+  static constexpr int N = 2048, M = 1024, TPF = 32;
+  static constexpr int NW = 16, THREADS = 512, GROUPS = 4, F = 16;  // frames per CTA tile
+  static constexpr uint32_t IMG = 128 * 128;      // one A image: 128 rows x 64 fp16 (16 KB)
+  static constexpr uint32_t FBUF = 33 * 32 * 8;   // one frame's padded spectrum + part slots (bytes)
+  static constexpr uint32_t REGION = 34 * 1024;   // per group: A hi + lo, later 4 spectra (1024-aligned)
+  static constexpr uint32_t BIMG = 64 * 128;      // one B image: 64 rows x 64 fp16 (8 KB)
+  static constexpr int MEL_SMEM_MAX = 8192;       // packed weights staged up to this many floats
+};
+static_assert(4 * TcShape::FBUF <= TcShape::REGION && 2 * TcShape::IMG <= TcShape::REGION, "group region");
+
+struct TcSmem {
+  uint32_t region, b, tw2, win, rs, mel, bar, taddr, total;
+};
+__host__ __device__ inline TcSmem tc_smem_layout(int n_mels, bool lanes, int nnz) {
+  using S = TcShape;
+  TcSmem L{};
+  uint32_t p = 0;
+  L.region = p;
+  p += S::GROUPS * S::REGION;
+  L.b = p;
+  p += 2 * S::BIMG;
+  L.tw2 = p;
+  p += 31 * S::TPF * 8;
+  L.win = p;
+  p += S::N * 4;
+  L.rs = p;
+  p += 16 * 32 * 8;
+  L.mel = p;
+  if (lanes)
+    p += (uint32_t)(align16(4 * (size_t)n_mels) + 8 * S::TPF + 33 * S::TPF * 8);
+  else
+    p += (uint32_t)(16 * (size_t)n_mels + (nnz <= S::MEL_SMEM_MAX ? align16(4 * (size_t)nnz) : 0));
+  p = (p + 15u) & ~15u;
+  L.bar = p;  // per group: GEMM 1 done, GEMM 2 done; then the exit barrier
+  p += 8 * (2 * S::GROUPS + 1);
+  p = (p + 15u) & ~15u;
+  L.taddr = p;
+  p += 16;
+  L.total = p + 1024;  // slack to align the base to 1024 bytes
+  return L;
+}
+
+// Named barrier over the 128 threads of group g (ids 1..4), returning whether
+// any of them passed `pred`.
+__device__ __forceinline__ bool group_sync_or(int g, bool pred) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, %2, 128, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)pred), "r"(g + 1)
+      : "memory");
+  return r != 0;
+}
+
+// Two fp16 parts of 8 floats (|x| < 1), packed for one 16-byte store each.
+// The hi part is x rounded to 11 significant bits in the float32 domain
+// (integer add and mask on the bits), so lo = x - hi is exact in float32 and
+// no fp16 value is converted back: only the two packing conversions remain.
+// (hi converts to fp16 exactly unless it falls below fp16's normal range,
+// where the error is at most 2^-25, far below the frame's largest sample.)
+__device__ __forceinline__ void split8_half(const float *x, uint4 &hi, uint4 &lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float h0 = __uint_as_float((__float_as_uint(x[2 * i]) + 0x1000u) & 0xFFFFE000u);
+    const float h1 = __uint_as_float((__float_as_uint(x[2 * i + 1]) + 0x1000u) & 0xFFFFE000u);
+    const __half2 a = __floats2half2_rn(h0, h1);
+    const __half2 b = __floats2half2_rn(x[2 * i] - h0, x[2 * i + 1] - h1);
+    h[i] = *reinterpret_cast<const uint32_t *>(&a);
+    l[i] = *reinterpret_cast<const uint32_t *>(&b);
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+__global__ void __launch_bounds__(TcShape::THREADS, 1) frame_tc_kernel(FrontArgs a) {
+  using S = TcShape;
+  constexpr int N = S::N, M = S::M, TPF = S::TPF;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char tc_raw[];
+  const uint32_t raw = smem_u32(tc_raw);
+  unsigned char *sm = tc_raw + (((raw + 1023u) & ~1023u) - raw);
+  const int nmel = a.n_mels;
+  const bool lanes = a.mel_lane_ok != 0;
+  const bool mel_in_smem = a.mel_nnz <= S::MEL_SMEM_MAX;
+  const TcSmem Ly = tc_smem_layout(nmel, lanes, a.mel_nnz);
+  cpx *tw2 = reinterpret_cast<cpx *>(sm + Ly.tw2);      // W_M^(j k1), [k1-1][j]
+  float *win_s = reinterpret_cast<float *>(sm + Ly.win);  // analysis window, halved
+  cpx *rs_tw = reinterpret_cast<cpx *>(sm + Ly.rs);     // real-split twiddles [32 i + l]
+  unsigned char *mp = sm + Ly.mel;
+  int *band_s = reinterpret_cast<int *>(mp);
+  int2 *lane_s = reinterpret_cast<int2 *>(mp + align16(4 * (size_t)nmel));
+  float2 *lw_s = reinterpret_cast<float2 *>(mp + align16(4 * (size_t)nmel) + 8 * TPF);
+  int4 *mel_s = reinterpret_cast<int4 *>(mp);
+  float *melw_s = reinterpret_cast<float *>(mp + 16 * (size_t)nmel);
+  const uint32_t bar0 = smem_u32(sm + Ly.bar);
+  uint32_t *taddr_s = reinterpret_cast<uint32_t *>(sm + Ly.taddr);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = warp >> 2, w4 = warp & 3;  // MMA group, frame within the group
+  const float2 *twq = a.tw_split;
+  unsigned char *region = sm + Ly.region + g * S::REGION;
+  const uint32_t a_hi = smem_u32(region), a_lo = a_hi + S::IMG;
+  const uint32_t b_hi = smem_u32(sm + Ly.b), b_lo = b_hi + S::BIMG;
+  const uint32_t bar_g1 = bar0 + 16u * (uint32_t)g, bar_g2 = bar_g1 + 8u, bar_fin = bar0 + 16u * S::GROUPS;
+
+  // ---- tables: the real-form 32-point DFT as fp16 hi/lo images (float64),
+  // B[n][k] for output n = 32 c_out + k' and input k = 32 c_in + n'
+  for (int i = tid; i < 64 * 64; i += S::THREADS) {
+    const int n = i >> 6, k = i & 63;
+    const int co = n >> 5, ci = k >> 5;
+    double sn, cs;
+    sincospi(2.0 * (double)(((n & 31) * (k & 31)) & 31) / 32.0, &sn, &cs);
+    const double v = (co == ci) ? cs : (co == 0 ? sn : -sn);
+    const __half hi = __double2half(v);
+    const __half lo = __double2half(v - (double)__half2float(hi));
+    *reinterpret_cast<__half *>(sm + Ly.b + sw128(n, k)) = hi;
+    *reinterpret_cast<__half *>(sm + Ly.b + S::BIMG + sw128(n, k)) = lo;
+  }
+  for (int i = tid; i < 31 * TPF; i += S::THREADS) {
+    const int k1 = i / TPF + 1, j = i - (k1 - 1) * TPF;
+    tw2[i] = root_q(twq, 2 * j * k1, N);
+  }
+  for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the warp kernel
+    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
+    reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
+  }
+  for (int i = tid; i < 16 * 32; i += S::THREADS) rs_tw[i] = root_q(twq, (i & 31) + 32 * (i >> 5), N);
+  if (lanes) {
+    for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
+    for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
+    for (int i = tid; i < 33 * TPF; i += S::THREADS) lw_s[i] = __ldg(a.mel_lw + i);
+  } else {
+    for (int i = tid; i < nmel; i += S::THREADS) mel_s[i] = __ldg(a.mel_info + i);
+    if (mel_in_smem)
+      for (int i = tid; i < a.mel_nnz; i += S::THREADS) melw_s[i] = __ldg(a.mel_pw + i);
+  }
+  const float *melw = mel_in_smem ? melw_s : a.mel_pw;
+  if (tid == 0) {
+    for (int q = 0; q < 2 * S::GROUPS; q++) mbar_init(bar0 + 8u * q, 1);
+    mbar_init(bar0 + 8u * (2 * S::GROUPS), S::GROUPS);  // one final commit per group
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
+                 "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();  // the B images are read by the tensor core
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *taddr_s;
+  const uint32_t acc = tmem + (uint32_t)(64 * g);               // this group's 64 columns
+  const uint32_t tl = acc + ((uint32_t)(32 * w4) << 16);         // this warp's lane quarter
+  constexpr uint32_t kId1 = idesc_f16kind<true>(64, 128, false);  // A K-major
+  constexpr uint32_t kId2 = idesc_f16kind<true>(64, 128, true);   // A MN-major
+  const bool issuer = (w4 == 0) && (lane == 0);
+
+  float *P = reinterpret_cast<float *>(region + w4 * S::FBUF);
+  const float ref_db = 10.0f * log10f(a.ref);
+  const int total = a.total_tiles;
+  const int t_begin = (int)((long long)blockIdx.x * total / gridDim.x);
+  const int t_end = (int)((long long)(blockIdx.x + 1) * total / gridDim.x);
+  int cur = -1;
+  float vmax = -INFINITY;
+  uint32_t it = 0;
+  bool failed = false;
+
+  for (int tile = t_begin; tile < t_end; tile++, it++) {
+    const int c = __ldg(a.tile_clip + tile);
+    if (c != cur) {  // warp-uniform: every frame of a tile belongs to one clip
+      float m = vmax;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+      if (lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+      cur = c;
+      vmax = -INFINITY;
+    }
+    const ClipDesc cd = load_clip(a.clips + c);
+    const int t = (tile - cd.tile_base) * S::F + 4 * g + w4;
+    const bool valid = t < cd.n_frames;  // warp-uniform; a frame past the clip computes zeros
+    const long long s0 = (long long)t * a.hop - a.pad;
+    const float *sig = a.signal + cd.sig_off;
+
+    // ---- gather + window: v[r] = (x[2n], x[2n+1]) w / 2 for n = lane + 32 r
+    cpx v[32];
+    if (!valid) {
+#pragma unroll
+      for (int r = 0; r < 32; r++) v[r] = {0.0f, 0.0f};
+    } else if (s0 >= 0 && s0 + N <= cd.length) {
+      const float *base = sig + s0 + 2 * lane;
+      if (((cd.sig_off + s0) & 1) == 0) {
+#pragma unroll
+        for (int r = 0; r < 32; r++) {
+          const float2 x = __ldg(reinterpret_cast<const float2 *>(base + 2 * TPF * r));
+          v[r] = {x.x, x.y};
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < 32; r++) v[r] = {__ldg(base + 2 * TPF * r), __ldg(base + 2 * TPF * r + 1)};
+      }
+    } else {
+      cpx tmp[32];
+      gather_edge(tmp, sig, s0 + 2 * lane, cd.length, a.pad_mode, 2 * TPF);
+#pragma unroll
+      for (int r = 0; r < 32; r++) v[r] = tmp[r];
+    }
+    float mx = 0.0f;
+    {
+      const float2 *wb = reinterpret_cast<const float2 *>(win_s) + lane;
+#pragma unroll
+      for (int r = 0; r < 32; r++) {
+        const float2 w = wb[TPF * r];
+        v[r].x *= w.x;
+        v[r].y *= w.y;
+        mx = fmaxf(mx, fmaxf(fabsf(v[r].x), fabsf(v[r].y)));  // NaNs are ignored here
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+    // 2^-e with the frame's largest windowed sample in [0.5, 1); 1 for a frame
+    // of zeros or one with an infinite sample
+    int e = 0;
+    if (mx > 0.0f && mx <= 3.402823466e38f) e = min(60, max(-60, ilogbf(mx) + 1));
+    const float sc = __int_as_float((127 - e) << 23);
+    const float isc2 = __int_as_float((127 + 2 * e) << 23);
+
+    // ---- GEMM 1's A: row 32 w4 + lane, K = [re z | im z] over n2 (K-major)
+    {
+      const int row = 32 * w4 + lane;
+#pragma unroll
+      for (int c8 = 0; c8 < 8; c8++) {
+        float xs[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+          const cpx z = v[(c8 & 3) * 8 + u];
+          xs[u] = (c8 < 4 ? z.x : z.y) * sc;
+        }
+        uint4 hi, lo;
+        split8_half(xs, hi, lo);
+        const uint32_t off = sw128(row, 8 * c8);
+        *reinterpret_cast<uint4 *>(region + off) = hi;
+        *reinterpret_cast<uint4 *>(region + S::IMG + off) = lo;
+      }
+    }
+    fence_proxy_async_smem();
+    group_sync_or(g, false);
+    if (issuer) {
+      tc_fence_after();
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint64_t ah = desc_sw128(a_hi + 32u * k), al = desc_sw128(a_lo + 32u * k);
+        const uint64_t bh = desc_sw128(b_hi + 32u * k), bl = desc_sw128(b_lo + 32u * k);
+        umma_f16kind(acc, ah, bh, kId1, k > 0 ? 1u : 0u);
+        umma_f16kind(acc, ah, bl, kId1, 1u);
+        umma_f16kind(acc, al, bh, kId1, 1u);
+      }
+      umma_commit(bar_g1);
+    }
+    bool ok = mbar_wait_bounded(bar_g1, it & 1u);
+    tc_fence_after();
+
+    // ---- GEMM 1's result: lane n1 holds Y[n1][k2] (columns k2 and 32 + k2)
+    float y[64];  // [re | im]
+    if (ok) {
+      tmem_ld64(tl, y);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 64; q++) y[q] = 0.0f;
+    }
+    float *yr = y, *yi = y + 32;
+    // twiddle W_M^(n1 k2)
+#pragma unroll
+    for (int k2 = 1; k2 < 32; k2++) {
+      const cpx r = cmul(cpx{yr[k2], yi[k2]}, tw2[(k2 - 1) * TPF + lane]);
+      yr[k2] = r.x;
+      yi[k2] = r.y;
+    }
+    // ---- GEMM 2's A (MN-major): K-rows n1 (re) and 32 + n1 (im), M = 32 w4 + k2;
+    // atoms of 64 M x 8 K-rows, 1024 bytes apart along M, 2048 along K
+    {
+      const uint32_t iblk = (uint32_t)(w4 >> 1) * 1024u;
+      const int cm0 = 4 * (w4 & 1);
+#pragma unroll
+      for (int part = 0; part < 2; part++) {
+        const int kidx = part * 32 + lane;
+        const uint32_t kbase = (uint32_t)(kidx >> 3) * 2048u + iblk + (uint32_t)(kidx & 7) * 128u;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          uint4 hi, lo;
+          split8_half(part ? yi + 8 * q : yr + 8 * q, hi, lo);
+          const uint32_t off = kbase + ((uint32_t)((cm0 + q) ^ (kidx & 7)) << 4);
+          *reinterpret_cast<uint4 *>(region + off) = hi;
+          *reinterpret_cast<uint4 *>(region + S::IMG + off) = lo;
+        }
+      }
+    }
+    tc_fence_before();  // this warp's tensor-memory loads are complete (tcgen05.wait::ld)
+    fence_proxy_async_smem();
+    if (group_sync_or(g, !ok)) {
+      failed = true;
+      break;
+    }
+    if (issuer) {
+      tc_fence_after();
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint64_t ah = desc_mn_sw128(a_hi + 4096u * k, 1024u, 2048u);
+        const uint64_t al = desc_mn_sw128(a_lo + 4096u * k, 1024u, 2048u);
+        const uint64_t bh = desc_sw128(b_hi + 32u * k), bl = desc_sw128(b_lo + 32u * k);
+        umma_f16kind(acc, ah, bh, kId2, k > 0 ? 1u : 0u);
+        umma_f16kind(acc, ah, bl, kId2, 1u);
+        umma_f16kind(acc, al, bh, kId2, 1u);
+      }
+      umma_commit(bar_g2);
+    }
+    ok = mbar_wait_bounded(bar_g2, it & 1u);
+    tc_fence_after();
+    // ---- GEMM 2's result: lane l = k2 of this frame holds v[k1] = Z[l + 32 k1]
+    if (ok) tmem_ld64(tl, y);
+#pragma unroll
+    for (int k1 = 0; k1 < 32; k1++) v[k1] = {y[k1], y[32 + k1]};
+    tc_fence_before();
+    // the spectra alias the A images: every MMA of the group has completed
+    // (each warp waited on GEMM 2's barrier), and no warp writes A before the
+    // barrier at the end of this tile
+
+    // ---- real split, P[k] = |X[k] sc|^2 (the window was halved), as the warp kernel (C == 1)
+    {
+      const int l = lane;
+      const int src = (32 - l) & 31;
+      cpx rcv[16];
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        rcv[q].x = __shfl_sync(FULL, v[16 + q].x, src);
+        rcv[q].y = __shfl_sync(FULL, v[16 + q].y, src);
+      }
+      const bool l0 = (l == 0);
+      float *Pa = P + l;
+      float *Pb = P + (M + TPF - 1 - l) + (l0 ? 1 : 0);
+      static_for<0, 16>([&](auto ki) {
+        constexpr int i = decltype(ki)::value;
+        const cpx za = v[i];
+        cpx zb;
+        if constexpr (i == 0) zb = l0 ? v[0] : rcv[15];
+        else zb = l0 ? rcv[16 - i] : rcv[15 - i];
+        const float ex = za.x + zb.x, ey = za.y - zb.y;
+        const float ox = za.y + zb.y, oy = zb.x - za.x;
+        const cpx w = rs_tw[32 * i + l];
+        const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
+        const float xr = ex + wr, xi = ey + wi;
+        const float yr2 = ex - wr, yi2 = ey - wi;
+        const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr2, yr2, yi2 * yi2);
+        Pa[33 * i] = p;
+        if constexpr (i == 0) Pb[l0 ? -1 : 0] = q;
+        else Pb[-33 * i] = q;
+      });
+      if (l0) P[M / 2 + TPF / 2] = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
+    }
+    __syncwarp();  // P complete
+
+    // ---- log-mel row + running clip max: band sums scaled back by 2^(2e)
+    float *dst = a.out + (cd.frame_off + t) * (long long)nmel;
+    const bool out = valid && ok;  // (a failed wait: the group stops at the barrier below)
+    if (lanes) {
+      float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
+      const int l = lane;
+      const int2 li = lane_s[l];
+      const unsigned fl = (unsigned)li.x;
+      int slot = li.y & 1023;
+      const float *pl = P + 33 * l;
+      const float2 *wl = lw_s + l;
+      float R = 0.0f, Fs = 0.0f, tot = 0.0f;
+#pragma unroll
+      for (int b = 0; b < 32; b++) {
+        const float p = pl[b];
+        const float2 w = wl[b * TPF];
+        tot = fmaf(p, 0.0f, tot);
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        if (fl & (1u << b)) {
+          parts[slot++] = make_float2(R, Fs);
+          R = 0.0f;
+          Fs = 0.0f;
+        }
+      }
+      if (l == TPF - 1) {
+        const float p = pl[32];
+        const float2 w = wl[32 * TPF];
+        tot = fmaf(p, 0.0f, tot);
+        R = fmaf(w.x, p, R);
+        Fs = fmaf(w.y, p, Fs);
+        parts[slot] = make_float2(R, Fs);
+      }
+      if (e > 53) {  // |X|^2 itself may overflow float32 only for samples this large
+        float pm = 0.0f;
+        for (int b = 0; b <= (l == TPF - 1 ? 32 : 31); b++) pm = fmaxf(pm, pl[b]);
+        tot = fmaf(pm * isc2, 0.0f, tot);
+      }
+      const bool bad = __ballot_sync(FULL, !isfinite(tot)) != 0;
+      if (l == 0) parts[li.y >> 16] = make_float2(0.0f, 0.0f);
+      __syncwarp();
+      const int kc = (li.y >> 10) & 63;
+      if (kc) {
+        const int h = l == TPF - 1 ? slot : slot - 1;
+        float2 hv = parts[h];
+        for (int j = 1; j <= kc; j++) {
+          const float2 pv = parts[h + j];
+          hv.x += pv.x;
+          hv.y += pv.y;
+        }
+        parts[h] = hv;
+      }
+      __syncwarp();
+      for (int m = l; m < nmel; m += TPF) {
+        const int bw = band_s[m];
+        float accm = (parts[bw & 4095].x + parts[(bw >> 12) & 4095].y) * isc2;
+        if (((bw >> 24) & 1) || bad) accm = __int_as_float(0x7fc00000);
+        const float val = db10_frame(accm, a.amin, ref_db);
+        if (out) {
+          dst[m] = val;
+          vmax = fmaxf(vmax, val);
+        }
+      }
+    } else {
+      float chk = 0.0f;
+      float pm = 0.0f;
+      for (int k = lane; k <= M; k += TPF) {
+        const float p = P[pad_bin<TPF>(k)];
+        chk = fmaf(p, 0.0f, chk);
+        pm = fmaxf(pm, p);
+      }
+      if (e > 53) chk = fmaf(pm * isc2, 0.0f, chk);
+      const bool bad = __ballot_sync(FULL, !isfinite(chk)) != 0;
+      for (int m = lane; m < nmel; m += TPF) {
+        const float accm = mel_dot_pad<TPF>(mel_s[m], melw, P, bad) * isc2;
+        const float val = db10_frame(accm, a.amin, ref_db);
+        if (out) {
+          dst[m] = val;
+          vmax = fmaxf(vmax, val);
+        }
+      }
+    }
+    // the spectra are read before the next tile's A overwrites them; a failed
+    // GEMM 2 wait ends the loop for the whole group here
+    if (group_sync_or(g, !ok)) {
+      failed = true;
+      break;
+    }
+  }
+  if (failed && lane == 0) atomicOr(a.err, 1u);
+  float m = vmax;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+  if (!failed && lane == 0 && cur >= 0 && m > -INFINITY) atomicMax(a.clip_max + cur, enc_f(m));
+  // every MMA this group issued has completed before tensor memory is released
+  if (issuer) {
+    umma_commit(bar_fin);  // arrives once the group's MMAs are done (one arrival per group issuer)
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (tid == 0) mbar_wait_bounded(bar_fin, 0u);
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+}
+
+cudaError_t launch_frontend_tc(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
+  using S = TcShape;
+  if (launched) *launched = 0;
+  if (a.total_tiles <= 0) return cudaSuccess;
+  if (!a.err) return cudaErrorInvalidValue;  // bounded waits report through the error word
+  const size_t smem = tc_smem_layout(a.n_mels, a.mel_lane_ok != 0, a.mel_nnz).total;
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  int per_sm = 1, sms = 148;
+  cudaError_t e =
+      persistent_geometry(reinterpret_cast<const void *>(frame_tc_kernel), S::THREADS, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = sms;  // one CTA per SM: 256 of the SM's 512 tensor-memory columns
+  if (grid_limit > 0 && grid > grid_limit) grid = grid_limit;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  frame_tc_kernel<<<(unsigned)grid, S::THREADS, smem, s>>>(a);
+  if (launched) *launched = (int)grid;
+  return cudaGetLastError();
 }
 
 static cudaError_t launch_warp2(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {

@@ -100,6 +100,8 @@ struct FrontArgs {
   // DFT_GEMM_F16X3 only: per frame (frame-major, as the log-mel rows) the
   // power of two the frame's samples are scaled by before the fp16 split
   float *frame_scale = nullptr;
+  // error word of kernels with bounded waits (tensor-core frame kernel)
+  unsigned *err = nullptr;
 };
 
 struct DctArgs {
@@ -152,6 +154,10 @@ int frames_per_tile(int log2n, int variant);
 int frame_variants(int log2n, int mode, int power_is_2);
 // Launch variant 3: the warp-per-frame kernel (MODE_MELDB, n_fft 256..2048).
 constexpr int kWarpVariant = 3;
+// Launch variant of the tensor-core frame kernel (n_fft 2048, MFCC path):
+// both 32-point DFT stages as fp16x3 tcgen05 GEMMs, 16 frames per tile.
+constexpr int kTcVariant = 5;
+constexpr int kTcFramesPerTile = 16;
 int warp_frames_per_tile(int log2n);  // 0 when the size has no warp kernel
 // Walking lanes of the filterbank walk (n_fft / 64, 32 bins each) for n_fft
 // 256..4096, else 0: the warp kernel's lanes (up to 2048), or the first
@@ -166,6 +172,7 @@ inline int mel_lane_tpf(int n_fft) {
 inline int mel_lane_max_slots(int tpf) {
   return tpf <= 0 ? 0 : (tpf <= 32 ? (33 * tpf - tpf * (32 / tpf - 1)) / 2 : 1024);
 }
+cudaError_t launch_frontend_tc(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched);
 cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,
                                  int *launched);
 // Stockham twiddle table length (entries) for log2(n_fft) >= 5.

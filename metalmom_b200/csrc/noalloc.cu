@@ -135,6 +135,7 @@ extern "C" MM_API int32_t mm_mfcc_noalloc(const float *d_signal, int64_t signal_
   int st = gpu_available();
   if (st != MM_OK) return st;
   g.variant = group_variant(g);
+  if (g.variant == kTcVariant) g.variant = kWarpVariant;  // its bounded waits report to a table's error word
 
   // Scratch needed beyond the tables: descriptors, clip max, log-mel rows.
   const int F = frames_per_tile(g.log2n, g.variant);

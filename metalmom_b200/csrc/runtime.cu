@@ -52,6 +52,8 @@ int group_variant(const Group &g) {
   if (g.dft_form != DFT_FFT_F32) return kDftVariant;
   const int nv = frame_variants(g.log2n, g.mode, g.power == 2.0f);
   const int v = tuned_variant(g.log2n);
+  if (v == kTcVariant)  // the tensor-core kernel: n_fft 2048 on the MFCC path only
+    return (g.log2n == 11 && g.mode == MODE_MELDB && g.power == 2.0f) ? kTcVariant : (nv > kWarpVariant ? kWarpVariant : 0);
   return (v >= 0 && v < nv) ? v : 0;
 }
 
@@ -124,11 +126,13 @@ const DevTables *get_tables(const Group &g, int *status) {
   e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
   if (e == cudaSuccess) {
     e = build_tables(*t, g.sr, g.n_fft, g.win, n_mels, g.fmin, g.fmax, n_mfcc, g.window_zero, s);
+    // the error word of the group's kernels with bounded waits (tensor-core
+    // DFT forms and frame kernel)
+    if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
     if (e == cudaSuccess && g.dft_form != DFT_FFT_F32) {
       t->dft = dft_shape(g.n_fft, g.win);
       e = cudaMalloc(&t->dft_basis, dft_basis_bytes(t->dft));
-      if (e == cudaSuccess) e = cudaMalloc(&t->dft_err, sizeof(unsigned));
-      if (e == cudaSuccess) e = cudaMemsetAsync(t->dft_err, 0, sizeof(unsigned), s);
       if (e == cudaSuccess)
         e = build_dft_basis(t->dft_basis, t->dft, g.win, g.window_zero, g.dft_form == DFT_GEMM_F16X3, s);
     }
@@ -303,6 +307,7 @@ cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, c
   a.ref = g.ref;
   a.out = (g.mode == MODE_MELDB) ? b.meldb : b.out;
   a.clip_max = b.clip_max;
+  a.err = t->dft_err;
   int grid = 0;
   if (g.dft_form == DFT_GEMM_F16X3 && g.mode == MODE_MELDB) {
     a.frame_scale = b.frame_scale;

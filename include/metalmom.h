@@ -328,6 +328,12 @@ MM_API int32_t mm_server_submit(mm_server server, const float* signal, int64_t l
  * cudaHostRegister) the upload runs at full PCIe speed with no host copy. */
 MM_API int32_t mm_server_submit_borrowed(mm_server server, const float* signal, int64_t length,
                                          const MMFrontEndParams* params, int64_t* request_id);
+/* n borrowed submits in one call (params: one struct per request).  On an
+ * error the requests before the failing one stay queued, the failing one and
+ * those after it get request_ids -1, and its status is returned. */
+MM_API int32_t mm_server_submit_borrowed_many(mm_server server, const float* const* signals,
+                                              const int64_t* lengths, int32_t n,
+                                              const MMFrontEndParams* params, int64_t* request_ids);
 /* MM_PENDING while running; otherwise moves the result ([rows, n_frames],
  * free with mm_buffer_free) into *out, or returns the request's error, and
  * forgets the request. */

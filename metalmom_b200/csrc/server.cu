@@ -585,6 +585,20 @@ int32_t mm_server_submit_borrowed(mm_server server, const float *signal, int64_t
   return submit_one(static_cast<Server *>(server), signal, length, params, request_id, true);
 }
 
+int32_t mm_server_submit_borrowed_many(mm_server server, const float *const *signals, const int64_t *lengths,
+                                       int32_t n, const MMFrontEndParams *params, int64_t *request_ids) {
+  if (!server || n < 0 || (n > 0 && (!signals || !lengths || !params || !request_ids))) return MM_ERR_INVALID_INPUT;
+  for (int32_t i = 0; i < n; i++) {
+    const int32_t st =
+        submit_one(static_cast<Server *>(server), signals[i], lengths[i], params + i, request_ids + i, true);
+    if (st != MM_OK) {
+      for (int32_t q = i; q < n; q++) request_ids[q] = -1;
+      return st;
+    }
+  }
+  return MM_OK;
+}
+
 int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer *out) {
   Server *srv = static_cast<Server *>(server);
   if (!srv || !out) return MM_ERR_INVALID_INPUT;

@@ -57,6 +57,32 @@ class Server:
         self._borrowed[int(rid[0])] = y
         return int(rid[0])
 
+    def submit_borrowed_many(self, clips, params_list) -> list:
+        """``submit_borrowed`` for many requests in one native call (the
+        client's per-request cost is one cffi argument each)."""
+        n = len(clips)
+        for y in clips:
+            if not (isinstance(y, np.ndarray) and y.dtype == np.float32 and y.flags.c_contiguous):
+                raise ValueError("submit_borrowed_many needs contiguous float32 arrays")
+        ptrs = ffi.new("const float*[]", [ffi.cast("const float*", y.ctypes.data) for y in clips])
+        lens = ffi.new("int64_t[]", [len(y) for y in clips])
+        ps = ffi.new("MMFrontEndParams[]", n)
+        cache = {}
+        for i, kw in enumerate(params_list):
+            key = tuple(sorted(kw.items()))
+            if key not in cache:
+                cache[key] = frontend_params(**kw)[0]
+            ps[i] = cache[key]
+        ids = ffi.new("int64_t[]", n)
+        st = lib.mm_server_submit_borrowed_many(self._srv, ptrs, lens, n, ps, ids)
+        out = [int(ids[i]) for i in range(n)]
+        for rid, y in zip(out, clips):
+            if rid >= 0:
+                self._borrowed[rid] = y
+        if st != 0:
+            raise RuntimeError(f"mm_server_submit_borrowed_many failed with status {st}")
+        return out
+
     def poll(self, rid: int):
         """The result if the request is done, else None."""
         out = ffi.new("MMBuffer*")

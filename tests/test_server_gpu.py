@@ -131,8 +131,9 @@ def test_poll_and_invalid_requests():
 
 
 def test_borrowed_submits_equal_copied_submits():
-    """mm_server_submit_borrowed reads the caller's (here pinned) buffers in
-    place: the results are bitwise those of copied submits."""
+    """mm_server_submit_borrowed (and its many-request form) reads the
+    caller's (here pinned) buffers in place: the results are bitwise those of
+    copied submits."""
     import torch
     reqs = _requests(12, seed=7)
     total = sum(len(y) for y, _ in reqs)
@@ -145,7 +146,10 @@ def test_borrowed_submits_equal_copied_submits():
     with M.Server(max_inflight=2, max_batch_clips=4) as srv:
         a = [srv.submit(y, **g) for y, g in reqs]
         b = [srv.submit_borrowed(v, **g) for v, (_, g) in zip(views, reqs)]
+        c = srv.submit_borrowed_many(views, [g for _, g in reqs])
         ra = [srv.result(i) for i in a]
         rb = [srv.result(i) for i in b]
-    for x, y in zip(ra, rb):
+        rc = [srv.result(i) for i in c]
+    for x, y, z in zip(ra, rb, rc):
         np.testing.assert_array_equal(x, y)
+        np.testing.assert_array_equal(x, z)

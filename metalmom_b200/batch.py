@@ -8,7 +8,7 @@ addresses and per-clip offsets the plan exposes.
 
 import numpy as np
 
-from ._buffer import buffer_to_numpy
+from ._bridge import take_buffer
 from ._native import ffi, lib
 
 
@@ -75,7 +75,7 @@ def mfcc_batch(clips, **params):
         status = lib.mm_mfcc_batch(ctx, ptrs, lens, n, p, outs)
         if status != 0:
             raise RuntimeError(f"mm_mfcc_batch failed with status {status}")
-        return [buffer_to_numpy(outs + i) for i in range(n)]
+        return [take_buffer(outs + i) for i in range(n)]
     finally:
         lib.mm_destroy(ctx)
 

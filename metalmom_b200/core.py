@@ -2,8 +2,15 @@
 
 import numpy as np
 
-from ._buffer import buffer_to_numpy
-from ._native import ffi, lib
+from ._bridge import bridge_call, float_ptr, stft_params
+from ._native import lib
+
+SR_UNUSED = 22050  # the bridge's STFT entry points take a sample rate they do not use
+
+
+def _defaults(n_fft, hop_length, win_length):
+    return (hop_length if hop_length is not None else n_fft // 4,
+            win_length if win_length is not None else n_fft)
 
 
 def stft(y, n_fft=2048, hop_length=None, win_length=None, center=True):
@@ -12,26 +19,9 @@ def stft(y, n_fft=2048, hop_length=None, win_length=None, center=True):
     Defaults as MetalMom's ``core.stft``: hop ``n_fft // 4``, window ``n_fft``,
     sample rate 22050 passed to the bridge (core.py:223-243).
     """
-    y = np.ascontiguousarray(y, dtype=np.float32)
-    hop = hop_length if hop_length is not None else n_fft // 4
-    win = win_length if win_length is not None else n_fft
-    ctx = lib.mm_init()
-    if ctx == ffi.NULL:
-        raise RuntimeError("Failed to initialize MetalMom context")
-    try:
-        params = ffi.new("MMSTFTParams*")
-        params.n_fft = n_fft
-        params.hop_length = hop
-        params.win_length = win
-        params.center = 1 if center else 0
-        out = ffi.new("MMBuffer*")
-        ptr = ffi.cast("const float*", y.ctypes.data)
-        status = lib.mm_stft(ctx, ptr, len(y), 22050, params, out)
-        if status != 0:
-            raise RuntimeError(f"mm_stft failed with status {status}")
-        return buffer_to_numpy(out)
-    finally:
-        lib.mm_destroy(ctx)
+    y, ptr = float_ptr(y)
+    hop, win = _defaults(n_fft, hop_length, win_length)
+    return bridge_call("mm_stft", lib.mm_stft, ptr, len(y), SR_UNUSED, stft_params(n_fft, hop, win, center))
 
 
 def stft_complex(y, n_fft=2048, hop_length=None, win_length=None, center=True):
@@ -42,27 +32,11 @@ def stft_complex(y, n_fft=2048, hop_length=None, win_length=None, center=True):
     hop ``n_fft // 4`` and window ``n_fft`` by default, DC and Nyquist real.
     ``istft(stft_complex(y))`` reconstructs ``y``.
     """
-    y = np.ascontiguousarray(y, dtype=np.float32)
-    hop = hop_length if hop_length is not None else n_fft // 4
-    win = win_length if win_length is not None else n_fft
-    ctx = lib.mm_init()
-    if ctx == ffi.NULL:
-        raise RuntimeError("Failed to initialize MetalMom context")
-    try:
-        params = ffi.new("MMSTFTParams*")
-        params.n_fft = n_fft
-        params.hop_length = hop
-        params.win_length = win
-        params.center = 1 if center else 0
-        out = ffi.new("MMBuffer*")
-        ptr = ffi.cast("const float*", y.ctypes.data)
-        status = lib.mm_stft_complex(ctx, ptr, len(y), 22050, params, out)
-        if status != 0:
-            raise RuntimeError(f"mm_stft_complex failed with status {status}")
-        inter = buffer_to_numpy(out)  # [n_freqs, n_frames, 2] float32
-        return np.ascontiguousarray(inter).view(np.complex64)[..., 0]
-    finally:
-        lib.mm_destroy(ctx)
+    y, ptr = float_ptr(y)
+    hop, win = _defaults(n_fft, hop_length, win_length)
+    inter = bridge_call("mm_stft_complex", lib.mm_stft_complex, ptr, len(y), SR_UNUSED,
+                        stft_params(n_fft, hop, win, center))  # [n_freqs, n_frames, 2] float32
+    return np.ascontiguousarray(inter).view(np.complex64)[..., 0]
 
 
 def istft(stft_matrix, hop_length=None, win_length=None, center=True, length=None):
@@ -75,19 +49,7 @@ def istft(stft_matrix, hop_length=None, win_length=None, center=True, length=Non
         stft_matrix = np.asarray(stft_matrix, dtype=np.complex64)
     n_freqs, n_frames = stft_matrix.shape
     n_fft = (n_freqs - 1) * 2
-    hop = hop_length if hop_length is not None else n_fft // 4
-    win = win_length if win_length is not None else n_fft
-    inter = np.ascontiguousarray(stft_matrix).view(np.float32)
-    ctx = lib.mm_init()
-    if ctx == ffi.NULL:
-        raise RuntimeError("Failed to initialize MetalMom context")
-    try:
-        out = ffi.new("MMBuffer*")
-        ptr = ffi.cast("const float*", inter.ctypes.data)
-        status = lib.mm_istft(ctx, ptr, inter.size, n_freqs, n_frames, 22050, hop, win,
-                              1 if center else 0, length if length is not None else 0, out)
-        if status != 0:
-            raise RuntimeError(f"mm_istft failed with status {status}")
-        return buffer_to_numpy(out)
-    finally:
-        lib.mm_destroy(ctx)
+    hop, win = _defaults(n_fft, hop_length, win_length)
+    inter, ptr = float_ptr(np.ascontiguousarray(stft_matrix).view(np.float32))
+    return bridge_call("mm_istft", lib.mm_istft, ptr, inter.size, n_freqs, n_frames, SR_UNUSED, hop, win,
+                       1 if center else 0, length if length is not None else 0)

@@ -8,22 +8,8 @@ the GPU.
 
 import numpy as np
 
-from ._buffer import buffer_to_numpy
+from ._bridge import bridge_call as _call
 from ._native import ffi, lib
-
-
-def _call(name, fn, *args):
-    ctx = lib.mm_init()
-    if ctx == ffi.NULL:
-        raise RuntimeError("Failed to initialize MetalMom context")
-    try:
-        out = ffi.new("MMBuffer*")
-        status = fn(ctx, *args, out)
-        if status != 0:
-            raise RuntimeError(f"{name} failed with status {status}")
-        return buffer_to_numpy(out)
-    finally:
-        lib.mm_destroy(ctx)
 
 
 def _columns(S, rows_axis):

@@ -9,7 +9,7 @@ separate CUDA streams.  ``submit`` returns a request id immediately;
 
 import numpy as np
 
-from ._buffer import buffer_to_numpy
+from ._bridge import take_buffer
 from ._native import ffi, lib
 from .batch import frontend_params
 
@@ -92,7 +92,7 @@ class Server:
         self._borrowed.pop(rid, None)
         if st != 0:
             raise RuntimeError(f"request {rid} failed with status {st}")
-        return buffer_to_numpy(out)
+        return take_buffer(out)
 
     def result(self, rid: int, timeout_ms: int = -1):
         """Wait for the request (``timeout_ms`` < 0: no limit) and return its MFCC."""
@@ -103,7 +103,7 @@ class Server:
         self._borrowed.pop(rid, None)
         if st != 0:
             raise RuntimeError(f"request {rid} failed with status {st}")
-        return buffer_to_numpy(out)
+        return take_buffer(out)
 
     def stats(self) -> dict:
         s = ffi.new("MMServerStats*")

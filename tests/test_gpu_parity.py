@@ -212,7 +212,7 @@ def test_int_input_and_short_signal():
 
 def test_buffer_freed_when_reshape_fails():
     from metalmom_b200._native import ffi, lib
-    from metalmom_b200._buffer import buffer_to_numpy
+    from metalmom_b200._bridge import take_buffer
     ctx = lib.mm_init()
     try:
         y = np.sin(np.arange(4096, dtype=np.float32))
@@ -224,7 +224,7 @@ def test_buffer_freed_when_reshape_fails():
         out.shape[0] = 9999
         out.shape[1] = 9999
         with pytest.raises(ValueError):
-            buffer_to_numpy(out)
+            take_buffer(out)
         assert out.data == ffi.NULL
     finally:
         lib.mm_destroy(ctx)

@@ -261,6 +261,11 @@ MM_API int32_t mm_plan_execute_timed(mm_plan plan, void* stream, int32_t slot);
 MM_API int32_t mm_plan_stage_ms(mm_plan plan, int32_t slot, float* ms3);
 /* Host buffers in and out: copies signals[i] into the device input, runs the
  * plan, copies every clip's result into outs[i] and synchronises. */
+/* Synchronises `stream` (NULL: the plan's own) and reports whether a bounded
+ * wait of a tensor-core kernel of the plan (DFT-as-GEMM forms, launch variant
+ * 5) ran out since the last report: MM_ERR_INTERNAL, else MM_OK.
+ * mm_plan_execute_host reports the same itself. */
+MM_API int32_t mm_plan_status(mm_plan plan, void* stream);
 MM_API int32_t mm_plan_execute_host(mm_plan plan, const float* const* signals, float* const* outs,
                              void* stream);
 

@@ -85,16 +85,7 @@ int run_batch(const Group &g_in, const float *const *signals, const int64_t *len
   if ((e = cudaMemcpyAsync(h, b.out, out_bytes, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_status(e);
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_status(e);
-  if (t->dft_err && (g.dft_form != DFT_FFT_F32 || g.variant == kTcVariant)) {
-    // a bounded wait of a tensor-core kernel ran out
-    unsigned flag = 0;
-    if ((e = cudaMemcpy(&flag, t->dft_err, sizeof(unsigned), cudaMemcpyDeviceToHost)) != cudaSuccess)
-      return cuda_status(e);
-    if (flag) {
-      cudaMemset(t->dft_err, 0, sizeof(unsigned));
-      return MM_ERR_INTERNAL;
-    }
-  }
+  if ((st = take_error_word(g, t)) != MM_OK) return st;  // a bounded wait of a tensor-core kernel ran out
   const int rows = output_rows(g);
   for (int i = 0; i < n; i++) {
     const size_t cnt = (size_t)rows * (size_t)L.clips[i].n_frames;

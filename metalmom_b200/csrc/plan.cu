@@ -386,7 +386,24 @@ int32_t mm_plan_execute_host(mm_plan plan, const float *const *signals, float *c
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, b.done, 0);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  return cuda_status(e);
+  if (e != cudaSuccess) return cuda_status(e);
+  for (const Sub &b : p->subs) {
+    const int st = take_error_word(b.g, b.t);
+    if (st != MM_OK) return st;
+  }
+  return MM_OK;
+}
+
+int32_t mm_plan_status(mm_plan plan, void *stream) {
+  Plan *p = as_plan(plan);
+  if (!p) return MM_ERR_INVALID_INPUT;
+  cudaError_t e = cudaStreamSynchronize(stream ? static_cast<cudaStream_t>(stream) : p->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  for (const Sub &b : p->subs) {
+    const int st = take_error_word(b.g, b.t);
+    if (st != MM_OK) return st;
+  }
+  return MM_OK;
 }
 
 }  // extern "C"

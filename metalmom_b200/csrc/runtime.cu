@@ -268,6 +268,16 @@ void pack_descriptors(const Layout &L, char *host) {
     memcpy(host + (o.dct_first - o.clips), L.dct_tile_first.data(), sizeof(int) * L.dct_tile_first.size());
 }
 
+int take_error_word(const Group &g, const DevTables *t) {
+  if (!t || !t->dft_err || (g.dft_form == DFT_FFT_F32 && g.variant != kTcVariant)) return MM_OK;
+  unsigned flag = 0;
+  cudaError_t e = cudaMemcpy(&flag, t->dft_err, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (!flag) return MM_OK;
+  cudaMemset(t->dft_err, 0, sizeof(unsigned));
+  return MM_ERR_INTERNAL;
+}
+
 cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, const DevBatch &b,
                           cudaStream_t s, cudaEvent_t *ev, int *n_launches) {
   cudaError_t e;

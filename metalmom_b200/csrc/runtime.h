@@ -88,6 +88,12 @@ void pack_descriptors(const Layout &L, char *host);
 
 // Enqueue the launch sequence of one batch.  `ev` may be null or point to 4
 // events recorded before/after the stages (frame kernel, DCT).
+// After the group's work has completed on the device: MM_ERR_INTERNAL (and
+// the word cleared) when a bounded wait of one of its tensor-core kernels ran
+// out, else MM_OK.  Reads the error word only for groups that launch such
+// kernels (the DFT-as-GEMM forms, the tensor-core frame kernel).
+int take_error_word(const Group &g, const DevTables *t);
+
 cudaError_t enqueue_batch(const Group &g, const Layout &L, const DevTables *t, const DevBatch &b,
                           cudaStream_t s, cudaEvent_t *ev, int *n_launches);
 

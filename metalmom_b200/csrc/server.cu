@@ -346,6 +346,11 @@ void Server::finish(Slot *s) {
     Clock::time_point t0 = Clock::now();
     ~Timer() { *acc += std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
   } timer{&finish_ms};
+  if (s->error == MM_OK) {  // a bounded wait of a tensor-core kernel of this batch ran out
+    int dev_st = MM_OK;
+    const DevTables *t = get_tables(s->g, &dev_st);
+    if (t) s->error = take_error_word(s->g, t);
+  }
   const int rows = output_rows(s->g);
   for (size_t i = 0; i < s->reqs.size(); i++) {
     Request *r = s->reqs[i];

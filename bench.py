@@ -397,7 +397,8 @@ def serving_leg(duration=3.0, rates=(50, 500, 2000), burst=2000, plain_s=2.0, n_
         res["saturation"] = {"requests": len(reqs), "audio_hours_per_s": audio_s / 3600.0 / wall, "wall_s": wall,
                              "p50_ms": st["latency_p50_ms"], "p99_ms": st["latency_p99_ms"],
                              "batches": st["batches_launched"], "h2d_bytes": int(sum(y.nbytes for y in pinned)),
-                             "submit_s": t_sub,
+                             "submit_s": t_sub, "scheduler_launch_ms": st["scheduler_launch_ms"],
+                             "scheduler_finish_ms": st["scheduler_finish_ms"],
                              "client": "mm_server_submit_borrowed_many: all requests from pinned host buffers in one call"}
     # the plain per-request form at its own saturation: mm_mfcc per request,
     # back to back, on the same requests

@@ -132,6 +132,16 @@ class PinnedPool {
   size_t cap() const { return cap_; }
 };
 
+// A batch's results in one pinned block from the pool: the device copies
+// them there, and each request's caller copies its own part out (outside the
+// server lock) and drops a reference; the last one returns the block.  The
+// scheduler thread then never copies results.
+struct ResultBlock {
+  float *data = nullptr;
+  int cls = 0;
+  std::atomic<int> refs{0};
+};
+
 struct Request {
   int64_t id = 0;
   Group g;
@@ -140,7 +150,9 @@ struct Request {
   int pin_cls = 0;
   std::vector<float> signal;  // ... or, when the pinned pool is full, a pageable copy ...
   const float *borrowed = nullptr;  // ... or the caller's own buffer (mm_server_submit_borrowed)
-  float *result = nullptr;  // malloc'd [rows x frames], handed to the caller
+  float *result = nullptr;  // malloc'd [rows x frames], handed to the caller ...
+  ResultBlock *block = nullptr;  // ... or its part of the batch's result block, copied out by the caller
+  const float *block_src = nullptr;
   long long rows = 0, frames = 0;
   int state = REQ_PENDING;
   int status = MM_OK;
@@ -166,6 +178,7 @@ struct Slot {
   char *arena = nullptr;
   size_t arena_size = 0;
   size_t sig_bytes = 0, desc_bytes = 0, out_bytes = 0;
+  ResultBlock *rblock = nullptr;  // this batch's results (else they land in `pinned`)
   int error = MM_OK;
 };
 
@@ -316,8 +329,21 @@ bool Server::admit_one(std::unique_lock<std::mutex> &lk) {
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(b.clips, h, slot->desc_bytes, cudaMemcpyHostToDevice, slot->stream);
       if (e == cudaSuccess) e = enqueue_batch(g, slot->L, t, b, slot->stream, nullptr, nullptr);
+      float *dst = reinterpret_cast<float *>(h);
+      int rcls = 0;
+      float *rb = pool->get(slot->out_bytes, &rcls);
+      if (rb) {
+        slot->rblock = new (std::nothrow) ResultBlock();
+        if (slot->rblock) {
+          slot->rblock->data = rb;
+          slot->rblock->cls = rcls;
+          dst = rb;
+        } else {
+          pool->put(rb, rcls);
+        }
+      }
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(h, b.out, slot->out_bytes, cudaMemcpyDeviceToHost, slot->stream);
+        e = cudaMemcpyAsync(dst, b.out, slot->out_bytes, cudaMemcpyDeviceToHost, slot->stream);
     }
     if (e != cudaSuccess) st = cuda_status(e);
   }
@@ -364,7 +390,11 @@ void Server::finish(Slot *s) {
       continue;
     }
     const size_t cnt = (size_t)rows * (size_t)r->frames;
-    if (cnt) {
+    if (cnt && s->rblock) {  // the caller copies its part out of the block
+      r->block = s->rblock;
+      r->block_src = s->rblock->data + s->L.clips[i].out_off;
+      s->rblock->refs.fetch_add(1);
+    } else if (cnt) {
       r->result = (float *)malloc(sizeof(float) * cnt);
       if (!r->result) {
         r->state = REQ_FAILED;
@@ -386,6 +416,11 @@ void Server::finish(Slot *s) {
     r->borrowed = nullptr;
     std::vector<float>().swap(r->signal);
   }
+  if (s->rblock && s->rblock->refs.load() == 0) {  // no request took a part (or the batch failed)
+    pool->put(s->rblock->data, s->rblock->cls);
+    delete s->rblock;
+  }
+  s->rblock = nullptr;
   if (s->arena) cudaFreeAsync(s->arena, s->stream);
   s->arena = nullptr;
   in_use -= s->arena_size;
@@ -413,15 +448,37 @@ void Server::run() {
   }
 }
 
-// Moves a finished request's result into *out (or returns its error) and
-// forgets the request.  Called with mu held.
-int32_t deliver(Server *srv, Request *r, MMBuffer *out) {
-  const int32_t st = r->status;
-  if (r->state == REQ_DONE) {
-    fill_buffer(out, r->result, r->rows, r->frames);
-    r->result = nullptr;
+// Drops one reference to a result block; the last returns it to the pool.
+void release_block(Server *srv, ResultBlock *b) {
+  if (b && b->refs.fetch_sub(1) == 1) {
+    srv->pool->put(b->data, b->cls);
+    delete b;
   }
-  srv->reqs.erase(r->id);
+}
+
+// Moves a finished request's result into *out (or returns its error) and
+// deletes the request, which the caller has already taken out of srv->reqs
+// (under mu); runs without the lock, so the copy out of a result block does
+// not hold up the scheduler.
+int32_t deliver(Server *srv, Request *r, MMBuffer *out) {
+  int32_t st = r->status;
+  if (r->state == REQ_DONE) {
+    if (r->block) {
+      const size_t cnt = (size_t)r->rows * (size_t)r->frames;
+      float *data = (float *)malloc(sizeof(float) * cnt);
+      if (data) {
+        memcpy(data, r->block_src, sizeof(float) * cnt);
+        fill_buffer(out, data, r->rows, r->frames);
+      } else {
+        st = MM_ERR_ALLOC_FAILED;
+      }
+      release_block(srv, r->block);
+      r->block = nullptr;
+    } else {
+      fill_buffer(out, r->result, r->rows, r->frames);
+      r->result = nullptr;
+    }
+  }
   free(r->result);
   delete r;
   return st;
@@ -573,6 +630,7 @@ void mm_server_destroy(mm_server server) {
   }
   for (auto &kv : srv->reqs) {
     free(kv.second->result);
+    release_block(srv, kv.second->block);
     delete kv.second;
   }
   if (srv->mempool) cudaMemPoolDestroy(srv->mempool);
@@ -607,24 +665,32 @@ int32_t mm_server_submit_borrowed_many(mm_server server, const float *const *sig
 int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer *out) {
   Server *srv = static_cast<Server *>(server);
   if (!srv || !out) return MM_ERR_INVALID_INPUT;
-  std::lock_guard<std::mutex> lk(srv->mu);
-  auto it = srv->reqs.find(request_id);
-  if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
-  Request *r = it->second;
-  if (r->state == REQ_PENDING || r->state == REQ_RUNNING) return MM_PENDING;
+  Request *r = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(request_id);
+    if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
+    r = it->second;
+    if (r->state == REQ_PENDING || r->state == REQ_RUNNING) return MM_PENDING;
+    srv->reqs.erase(it);
+  }
   return deliver(srv, r, out);
 }
 
 int32_t mm_server_wait(mm_server server, int64_t request_id, int32_t timeout_ms, MMBuffer *out) {
   Server *srv = static_cast<Server *>(server);
   if (!srv || !out) return MM_ERR_INVALID_INPUT;
-  std::unique_lock<std::mutex> lk(srv->mu);
-  auto it = srv->reqs.find(request_id);
-  if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
-  Request *r = it->second;
-  auto ready = [r] { return r->state == REQ_DONE || r->state == REQ_FAILED; };
-  if (timeout_ms < 0) srv->done_cv.wait(lk, ready);
-  else if (!srv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return MM_PENDING;
+  Request *r = nullptr;
+  {
+    std::unique_lock<std::mutex> lk(srv->mu);
+    auto it = srv->reqs.find(request_id);
+    if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
+    r = it->second;
+    auto ready = [r] { return r->state == REQ_DONE || r->state == REQ_FAILED; };
+    if (timeout_ms < 0) srv->done_cv.wait(lk, ready);
+    else if (!srv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return MM_PENDING;
+    srv->reqs.erase(request_id);
+  }
   return deliver(srv, r, out);
 }
 

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <tuple>
 
+#include "async_copy.cuh"
 #include "fft_radix.cuh"
 #include "frame_common.cuh"
 #include "kernels.h"
@@ -1618,6 +1619,156 @@ __global__ void __launch_bounds__(256, 3) dct_fold_kernel(DctArgs a) {
   }
 }
 
+// The same folded product (128 bands, coefficient groups as in
+// dct_fold_kernel, the same summation order, so the same results bit for bit)
+// with fewer instructions per frame and the rows' latency hidden by copies:
+// - a tile's rows are copied straight into shared memory by cp.async (no
+//   registers in flight), two tile buffers, the next tile's copies issued
+//   before this one is folded;
+// - the floor and the even/odd fold run in place in shared memory: a thread
+//   takes float4 chunks j, 15 - j of a row and their mirrors 31 - j, 16 + j,
+//   reads all four, then writes e over chunks j, 15 - j and o over 16 + j,
+//   31 - j (the row becomes [e | o]);
+// - 128 threads, each two frames (lane, lane + 32) x KQ coefficients of its
+//   warp's group, so every basis read from shared memory feeds two frames.
+constexpr int kDct2Stride = 132;  // floats per staged row (16-byte aligned, conflict-free reads)
+
+template <int KQ>
+__global__ void __launch_bounds__(128, 3) dct_fold2_kernel(DctArgs a) {
+  constexpr int NM = 128, H = NM / 2, H4 = H / 4, TS = kDct2Stride;
+  extern __shared__ __align__(16) float dsm[];
+  float *buf0 = dsm;                  // [kDctTile][TS] x 2
+  float *bas = dsm + 2 * kDctTile * TS;  // [4*KQ][H]
+  const int tid = threadIdx.x, lane = tid & 31, kg = tid >> 5;
+  auto coef = [](int g, int q) { return g < 2 ? 2 * (KQ * g + q) : 2 * (KQ * (g - 2) + q) + 1; };
+  for (int i = tid; i < 4 * KQ * H; i += 128) {
+    const int row = i / H, n = i - row * H;
+    const int k = coef(row / KQ, row % KQ);
+    bas[i] = k < a.n_mfcc ? __ldg(a.basis + (long long)k * NM + n) : 0.0f;
+  }
+  int ti = blockIdx.x;
+  if (ti >= a.total_tiles) return;
+  // A tile's meta takes three dependent loads (tile -> clip -> descriptor and
+  // maximum); they are spread over the tile two ahead of the one multiplied:
+  // its tile words at the top, its clip's words after the fold, the meta put
+  // together after the product, so no warp waits on a chain of loads.
+  auto finish_meta = [&](int c, int tf, const ClipDesc &cd, unsigned cm) {
+    DctTileMeta m;
+    m.tf = tf;
+    m.nt = min(kDctTile, cd.n_frames - tf);
+    m.thr = a.top_db > 0.0f ? dec_f(cm) - a.top_db : -INFINITY;
+    m.src = reinterpret_cast<const float4 *>(a.mel_db + (cd.frame_off + tf) * (long long)NM);
+    m.out_off = cd.out_off;
+    m.T = cd.n_frames;
+    return m;
+  };
+  // rows r < nt of tile m into buffer b: chunk i = tid + 128 u is row i / 32, float4 i % 32
+  auto issue = [&](const DctTileMeta &m, float *b) {
+#pragma unroll
+    for (int u = 0; u < kDctTile * 32 / 128; u++) {
+      const int i = tid + 128 * u, r = i >> 5, c4 = i & 31;
+      if (r < m.nt) cp_async16(b + r * TS + 4 * c4, m.src + r * 32 + c4);
+    }
+    cp_async_commit();
+  };
+  const int G = gridDim.x;
+  DctTileMeta cur = dct_tile_meta(a, ti);
+  issue(cur, buf0);
+  DctTileMeta nxt = cur;
+  if (ti + G < a.total_tiles) nxt = dct_tile_meta(a, ti + G);
+  const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * H);
+  for (int k = 0; ti < a.total_tiles; ti += G, k++) {
+    float *b = buf0 + (k & 1) * kDctTile * TS;
+    const bool more = ti + G < a.total_tiles;
+    if (more) {
+      issue(nxt, buf0 + ((k + 1) & 1) * kDctTile * TS);  // that buffer was released at the end of tile k - 1
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    // tile words of the tile two ahead
+    const int t2 = ti + 2 * G;
+    const bool has2 = t2 < a.total_tiles;
+    int c2 = 0, f2 = 0;
+    if (has2) {
+      c2 = __ldg(a.tile_clip + t2);
+      f2 = __ldg(a.tile_first + t2);
+    }
+    __syncthreads();  // every thread's copies of this tile have landed
+    // floor + fold in place: unit i = tid + 128 u is row i / 8, chunk pair j = i % 8
+#pragma unroll
+    for (int u = 0; u < kDctTile * 8 / 128; u++) {
+      const int i = tid + 128 * u, r = i >> 3, j = i & 7;
+      if (r < cur.nt) {
+        float4 *row = reinterpret_cast<float4 *>(b + r * TS);
+        float4 A = row[j], Am = row[31 - j], B = row[15 - j], Bm = row[16 + j];
+        const float t = cur.thr;
+        A = make_float4(vthr(A.x, t), vthr(A.y, t), vthr(A.z, t), vthr(A.w, t));
+        Am = make_float4(vthr(Am.x, t), vthr(Am.y, t), vthr(Am.z, t), vthr(Am.w, t));
+        B = make_float4(vthr(B.x, t), vthr(B.y, t), vthr(B.z, t), vthr(B.w, t));
+        Bm = make_float4(vthr(Bm.x, t), vthr(Bm.y, t), vthr(Bm.z, t), vthr(Bm.w, t));
+        row[j] = make_float4(A.x + Am.w, A.y + Am.z, A.z + Am.y, A.w + Am.x);
+        row[16 + j] = make_float4(A.x - Am.w, A.y - Am.z, A.z - Am.y, A.w - Am.x);
+        row[15 - j] = make_float4(B.x + Bm.w, B.y + Bm.z, B.z + Bm.y, B.w + Bm.x);
+        row[31 - j] = make_float4(B.x - Bm.w, B.y - Bm.z, B.z - Bm.y, B.w - Bm.x);
+      }
+    }
+    // its clip's words
+    ClipDesc cd2{};
+    unsigned cm2 = 0;
+    if (has2) {
+      cd2 = load_clip(a.clips + c2);
+      cm2 = __ldg(a.clip_max + c2);
+    }
+    __syncthreads();
+    const float4 *t0 = reinterpret_cast<const float4 *>(b + lane * TS + (kg < 2 ? 0 : H));
+    const float4 *t1 = t0 + 32 * TS / 4;
+    float acc0[KQ], acc1[KQ];
+#pragma unroll
+    for (int q = 0; q < KQ; q++) acc0[q] = acc1[q] = 0.0f;
+#pragma unroll
+    for (int j = 0; j < H4; j++) {
+      const float4 d0 = t0[j], d1 = t1[j];
+#pragma unroll
+      for (int q = 0; q < KQ; q++) {
+        const float4 w = brow[q * H4 + j];
+        acc0[q] = fmaf(w.x, d0.x, acc0[q]);
+        acc0[q] = fmaf(w.y, d0.y, acc0[q]);
+        acc0[q] = fmaf(w.z, d0.z, acc0[q]);
+        acc0[q] = fmaf(w.w, d0.w, acc0[q]);
+        acc1[q] = fmaf(w.x, d1.x, acc1[q]);
+        acc1[q] = fmaf(w.y, d1.y, acc1[q]);
+        acc1[q] = fmaf(w.z, d1.z, acc1[q]);
+        acc1[q] = fmaf(w.w, d1.w, acc1[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < KQ; q++) {
+      const int kk = coef(kg, q);
+      if (kk < a.n_mfcc) {
+        float *o = a.out + cur.out_off + (long long)kk * cur.T + cur.tf;
+        if (lane < cur.nt) o[lane] = acc0[q];
+        if (lane + 32 < cur.nt) o[lane + 32] = acc1[q];
+      }
+    }
+    __syncthreads();  // this tile's buffer is free for the copies of tile k + 2
+    cur = nxt;
+    if (has2) nxt = finish_meta(c2, f2, cd2, cm2);
+  }
+}
+
+template <int KQ>
+static cudaError_t launch_dct_fold2_t(const DctArgs &a, cudaStream_t s) {
+  const size_t smem = sizeof(float) * ((size_t)2 * kDctTile * kDct2Stride + (size_t)4 * KQ * 64);
+  int per_sm = 1, sms = 148;
+  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(dct_fold2_kernel<KQ>), 128, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = (long long)sms * per_sm;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  dct_fold2_kernel<KQ><<<(unsigned)grid, 128, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 template <int KQ>
 static cudaError_t launch_dct_fold_t(const DctArgs &a, cudaStream_t s) {
   const size_t smem = sizeof(float) * ((size_t)4 * KQ * 64 + (size_t)kDctTile * dct_row_stride(128));
@@ -1671,14 +1822,14 @@ cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
   if (a.n_mfcc <= kDctKC && a.n_mels == 128) {
     switch ((a.n_mfcc + 3) / 4) {  // ceil(ceil(n_mfcc / 2) / 2)
-      case 1: return launch_dct_fold_t<1>(a, s);
-      case 2: return launch_dct_fold_t<2>(a, s);
-      case 3: return launch_dct_fold_t<3>(a, s);
-      case 4: return launch_dct_fold_t<4>(a, s);
-      case 5: return launch_dct_fold_t<5>(a, s);
-      case 6: return launch_dct_fold_t<6>(a, s);
-      case 7: return launch_dct_fold_t<7>(a, s);
-      default: return launch_dct_fold_t<8>(a, s);
+      case 1: return launch_dct_fold2_t<1>(a, s);
+      case 2: return launch_dct_fold2_t<2>(a, s);
+      case 3: return launch_dct_fold2_t<3>(a, s);
+      case 4: return launch_dct_fold2_t<4>(a, s);
+      case 5: return launch_dct_fold2_t<5>(a, s);
+      case 6: return launch_dct_fold2_t<6>(a, s);
+      case 7: return launch_dct_fold2_t<7>(a, s);
+      default: return launch_dct_fold2_t<8>(a, s);
     }
   }
   if (a.n_mfcc <= kDctKC && a.n_mels % 4 == 0 && a.n_mels <= 4 * kDctPipeVec * 256 / kDctTile) {

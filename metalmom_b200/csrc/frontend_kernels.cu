@@ -1521,107 +1521,11 @@ __global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
 // for odd k (cos(pi k (2(N-1-n)+1) / 2N) = (-1)^k cos(pi k (2n+1) / 2N)), so
 // with e_n = x_n + x_{N-1-n} and o_n = x_n - x_{N-1-n} (n < N/2) the even
 // coefficients are sum_n B[k][n] e_n and the odd ones sum_n B[k][n] o_n: half
-// the products and half the basis reads.  In the store phase lane l of a warp
-// holds float4 chunk l of a row and its mirror chunk 31 - l sits in lane l^31,
-// so the fold costs four shuffles per chunk; a tile row becomes [e | o].
-// Coefficient groups: kg 0, 1 take even k = 2 (KQ kg + q), kg 2, 3 odd
-// k = 2 (KQ (kg - 2) + q) + 1, so KQ = ceil(ceil(n_mfcc / 2) / 2).
-template <int KQ>
-__global__ void __launch_bounds__(256, 3) dct_fold_kernel(DctArgs a) {
-  constexpr int NM = 128, H = NM / 2, H4 = H / 4;
-  constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ __align__(16) float dsm[];
-  const int stride = dct_row_stride(NM);
-  float *bas = dsm;                // [4*KQ][H]: half basis rows of this CTA's coefficients
-  float *tile = dsm + 4 * KQ * H;  // [64][stride]: e | o per frame
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int fr = tid & (kDctTile - 1), kg = tid / kDctTile;
-  auto coef = [](int g, int q) { return g < 2 ? 2 * (KQ * g + q) : 2 * (KQ * (g - 2) + q) + 1; };
-  for (int i = tid; i < 4 * KQ * H; i += 256) {
-    const int row = i / H, n = i - row * H;
-    const int k = coef(row / KQ, row % KQ);
-    bas[i] = k < a.n_mfcc ? __ldg(a.basis + (long long)k * NM + n) : 0.0f;
-  }
-  const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * H);
-  const float4 *trow = reinterpret_cast<const float4 *>(tile + fr * stride + (kg < 2 ? 0 : H));
-  int ti = blockIdx.x;
-  if (ti >= a.total_tiles) return;
-  // chunk v of this thread: row warp + 8 v, float4 column lane (32 per row)
-  float4 pre[kDctPipeVec];
-  DctTileMeta cur = dct_tile_meta(a, ti);
-#pragma unroll
-  for (int v = 0; v < kDctPipeVec; v++) {
-    const int r = warp + 8 * v;
-    pre[v] = r < cur.nt ? __ldg(cur.src + r * (NM / 4) + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  for (; ti < a.total_tiles; ti += gridDim.x) {
-    __syncthreads();  // every thread is done with the previous tile in shared memory
-#pragma unroll
-    for (int v = 0; v < kDctPipeVec; v++) {
-      const int r = warp + 8 * v;  // warp-uniform
-      float4 x = pre[v];
-      if (r < cur.nt) {
-        x.x = vthr(x.x, cur.thr);
-        x.y = vthr(x.y, cur.thr);
-        x.z = vthr(x.z, cur.thr);
-        x.w = vthr(x.w, cur.thr);
-      }
-      float4 y;
-      y.x = __shfl_xor_sync(FULL, x.x, 31);
-      y.y = __shfl_xor_sync(FULL, x.y, 31);
-      y.z = __shfl_xor_sync(FULL, x.z, 31);
-      y.w = __shfl_xor_sync(FULL, x.w, 31);
-      float4 f;
-      int pos;
-      if (lane < 16) {  // e over chunk lane: x[4l + t] + x[N - 1 - 4l - t]
-        f = make_float4(x.x + y.w, x.y + y.z, x.z + y.y, x.w + y.x);
-        pos = lane;
-      } else {  // o over chunk 31 - l: mirror chunk (from lane 31 - l) minus this one reversed
-        f = make_float4(y.x - x.w, y.y - x.z, y.z - x.y, y.w - x.x);
-        pos = H4 + 31 - lane;
-      }
-      *reinterpret_cast<float4 *>(tile + r * stride + 4 * pos) = f;
-    }
-    __syncthreads();
-    const int nti = ti + gridDim.x;
-    DctTileMeta nxt = cur;
-    if (nti < a.total_tiles) {
-      nxt = dct_tile_meta(a, nti);
-#pragma unroll
-      for (int v = 0; v < kDctPipeVec; v++) {
-        const int r = warp + 8 * v;
-        pre[v] = r < nxt.nt ? __ldg(nxt.src + r * (NM / 4) + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-    }
-    float acc[KQ];
-#pragma unroll
-    for (int q = 0; q < KQ; q++) acc[q] = 0.0f;
-#pragma unroll
-    for (int j = 0; j < H4; j++) {
-      const float4 d = trow[j];
-#pragma unroll
-      for (int q = 0; q < KQ; q++) {
-        const float4 b = brow[q * H4 + j];
-        acc[q] = fmaf(b.x, d.x, acc[q]);
-        acc[q] = fmaf(b.y, d.y, acc[q]);
-        acc[q] = fmaf(b.z, d.z, acc[q]);
-        acc[q] = fmaf(b.w, d.w, acc[q]);
-      }
-    }
-    if (fr < cur.nt) {
-#pragma unroll
-      for (int q = 0; q < KQ; q++) {
-        const int k = coef(kg, q);
-        if (k < a.n_mfcc) a.out[cur.out_off + (long long)k * cur.T + cur.tf + fr] = acc[q];
-      }
-    }
-    cur = nxt;
-  }
-}
-
-// The same folded product (128 bands, coefficient groups as in
-// dct_fold_kernel, the same summation order, so the same results bit for bit)
-// with fewer instructions per frame and the rows' latency hidden by copies:
+// the products and half the basis reads.
+// Coefficient groups (one per warp): kg 0, 1 take even k = 2 (KQ kg + q),
+// kg 2, 3 odd k = 2 (KQ (kg - 2) + q) + 1, so KQ = ceil(ceil(n_mfcc / 2) / 2).
+// Per tile of 64 frames (the summation order of the other DCT kernels: float4
+// chunk by chunk, x, y, z, w):
 // - a tile's rows are copied straight into shared memory by cp.async (no
 //   registers in flight), two tile buffers, the next tile's copies issued
 //   before this one is folded;
@@ -1766,18 +1670,6 @@ static cudaError_t launch_dct_fold2_t(const DctArgs &a, cudaStream_t s) {
   long long grid = (long long)sms * per_sm;
   if (grid > a.total_tiles) grid = a.total_tiles;
   dct_fold2_kernel<KQ><<<(unsigned)grid, 128, smem, s>>>(a);
-  return cudaGetLastError();
-}
-
-template <int KQ>
-static cudaError_t launch_dct_fold_t(const DctArgs &a, cudaStream_t s) {
-  const size_t smem = sizeof(float) * ((size_t)4 * KQ * 64 + (size_t)kDctTile * dct_row_stride(128));
-  int per_sm = 1, sms = 148;
-  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(dct_fold_kernel<KQ>), 256, smem, &per_sm, &sms);
-  if (e != cudaSuccess) return e;
-  long long grid = (long long)sms * per_sm;
-  if (grid > a.total_tiles) grid = a.total_tiles;
-  dct_fold_kernel<KQ><<<(unsigned)grid, 256, smem, s>>>(a);
   return cudaGetLastError();
 }
 

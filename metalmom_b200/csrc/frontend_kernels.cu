@@ -1536,13 +1536,16 @@ __global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
 // - 128 threads, each two frames (lane, lane + 32) x KQ coefficients of its
 //   warp's group, so every basis read from shared memory feeds two frames.
 constexpr int kDct2Stride = 132;  // floats per staged row (16-byte aligned, conflict-free reads)
+// Tile buffers in the copy ring: two (3 CTAs per SM) measured 0.0618 ms per
+// bench step against 0.0677 ms for three (2 CTAs per SM).
+constexpr int kDctFoldStages = 2;
 
-template <int KQ>
-__global__ void __launch_bounds__(128, 3) dct_fold2_kernel(DctArgs a) {
+template <int KQ, int S>
+__global__ void __launch_bounds__(128, S == 2 ? 3 : 2) dct_fold2_kernel(DctArgs a) {
   constexpr int NM = 128, H = NM / 2, H4 = H / 4, TS = kDct2Stride;
   extern __shared__ __align__(16) float dsm[];
-  float *buf0 = dsm;                  // [kDctTile][TS] x 2
-  float *bas = dsm + 2 * kDctTile * TS;  // [4*KQ][H]
+  float *buf0 = dsm;                     // [kDctTile][TS] x S
+  float *bas = dsm + S * kDctTile * TS;  // [4*KQ][H]
   const int tid = threadIdx.x, lane = tid & 31, kg = tid >> 5;
   auto coef = [](int g, int q) { return g < 2 ? 2 * (KQ * g + q) : 2 * (KQ * (g - 2) + q) + 1; };
   for (int i = tid; i < 4 * KQ * H; i += 128) {
@@ -1553,7 +1556,7 @@ __global__ void __launch_bounds__(128, 3) dct_fold2_kernel(DctArgs a) {
   int ti = blockIdx.x;
   if (ti >= a.total_tiles) return;
   // A tile's meta takes three dependent loads (tile -> clip -> descriptor and
-  // maximum); they are spread over the tile two ahead of the one multiplied:
+  // maximum); they are spread over the tile S ahead of the one multiplied:
   // its tile words at the top, its clip's words after the fold, the meta put
   // together after the product, so no warp waits on a chain of loads.
   auto finish_meta = [&](int c, int tf, const ClipDesc &cd, unsigned cm) {
@@ -1576,22 +1579,31 @@ __global__ void __launch_bounds__(128, 3) dct_fold2_kernel(DctArgs a) {
     cp_async_commit();
   };
   const int G = gridDim.x;
-  DctTileMeta cur = dct_tile_meta(a, ti);
-  issue(cur, buf0);
-  DctTileMeta nxt = cur;
-  if (ti + G < a.total_tiles) nxt = dct_tile_meta(a, ti + G);
+  // m[0]: this tile; m[s]: the tile s ahead (copies issued for s < S - 1)
+  DctTileMeta m[S];
+  m[0] = dct_tile_meta(a, ti);
+  issue(m[0], buf0);
+#pragma unroll
+  for (int q = 1; q < S; q++) {
+    m[q] = m[q - 1];
+    if (ti + q * G < a.total_tiles) {
+      m[q] = dct_tile_meta(a, ti + q * G);
+      if (q < S - 1) issue(m[q], buf0 + q * kDctTile * TS);
+    }
+  }
   const float4 *brow = reinterpret_cast<const float4 *>(bas + kg * KQ * H);
   for (int k = 0; ti < a.total_tiles; ti += G, k++) {
-    float *b = buf0 + (k & 1) * kDctTile * TS;
-    const bool more = ti + G < a.total_tiles;
-    if (more) {
-      issue(nxt, buf0 + ((k + 1) & 1) * kDctTile * TS);  // that buffer was released at the end of tile k - 1
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
-    // tile words of the tile two ahead
-    const int t2 = ti + 2 * G;
+    const DctTileMeta &cur = m[0];
+    float *b = buf0 + (k % S) * kDctTile * TS;
+    // copies of the tile S - 1 ahead into the buffer released at the end of
+    // tile k - 1, then wait for this tile's (tiles after it stay in flight)
+    const int ahead = min(S - 1, (a.total_tiles - 1 - ti) / G);
+    if (ahead == S - 1) issue(m[S - 1], buf0 + ((k + S - 1) % S) * kDctTile * TS);
+    if (S == 3 && ahead >= 2) cp_async_wait<2>();
+    else if (ahead >= 1) cp_async_wait<1>();
+    else cp_async_wait<0>();
+    // tile words of the tile S ahead
+    const int t2 = ti + S * G;
     const bool has2 = t2 < a.total_tiles;
     int c2 = 0, f2 = 0;
     if (has2) {
@@ -1655,22 +1667,29 @@ __global__ void __launch_bounds__(128, 3) dct_fold2_kernel(DctArgs a) {
         if (lane + 32 < cur.nt) o[lane + 32] = acc1[q];
       }
     }
-    __syncthreads();  // this tile's buffer is free for the copies of tile k + 2
-    cur = nxt;
-    if (has2) nxt = finish_meta(c2, f2, cd2, cm2);
+    __syncthreads();  // this tile's buffer is free for the copies of tile k + S
+#pragma unroll
+    for (int q = 0; q < S - 1; q++) m[q] = m[q + 1];
+    if (has2) m[S - 1] = finish_meta(c2, f2, cd2, cm2);
   }
+}
+
+template <int KQ, int S>
+static cudaError_t launch_dct_fold2_s(const DctArgs &a, cudaStream_t s) {
+  const size_t smem = sizeof(float) * ((size_t)S * kDctTile * kDct2Stride + (size_t)4 * KQ * 64);
+  int per_sm = 1, sms = 148;
+  cudaError_t e =
+      persistent_geometry(reinterpret_cast<const void *>(dct_fold2_kernel<KQ, S>), 128, smem, &per_sm, &sms);
+  if (e != cudaSuccess) return e;
+  long long grid = (long long)sms * per_sm;
+  if (grid > a.total_tiles) grid = a.total_tiles;
+  dct_fold2_kernel<KQ, S><<<(unsigned)grid, 128, smem, s>>>(a);
+  return cudaGetLastError();
 }
 
 template <int KQ>
 static cudaError_t launch_dct_fold2_t(const DctArgs &a, cudaStream_t s) {
-  const size_t smem = sizeof(float) * ((size_t)2 * kDctTile * kDct2Stride + (size_t)4 * KQ * 64);
-  int per_sm = 1, sms = 148;
-  cudaError_t e = persistent_geometry(reinterpret_cast<const void *>(dct_fold2_kernel<KQ>), 128, smem, &per_sm, &sms);
-  if (e != cudaSuccess) return e;
-  long long grid = (long long)sms * per_sm;
-  if (grid > a.total_tiles) grid = a.total_tiles;
-  dct_fold2_kernel<KQ><<<(unsigned)grid, 128, smem, s>>>(a);
-  return cudaGetLastError();
+  return launch_dct_fold2_s<KQ, kDctFoldStages>(a, s);
 }
 
 template <int KQ>

@@ -304,7 +304,9 @@ typedef struct {
     int64_t device_budget_bytes; /* device memory of the batches in flight; <= 0: 40 GiB */
     int32_t max_batch_clips;     /* <= 0: 256 */
     int32_t max_inflight;        /* batches on the device at once; <= 0: 4 (at most 64) */
-    int64_t host_pinned_bytes;   /* pinned host memory for queued samples; <= 0: 8 GiB */
+    int64_t host_pinned_bytes;   /* pinned host memory for queued samples and batch results; <= 0: 8 GiB
+                                    (past it, samples wait in pageable copies and results go
+                                    through the batch slot's staging) */
 } MMServerConfig;
 
 typedef struct {

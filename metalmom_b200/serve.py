@@ -22,11 +22,12 @@ STAT_KEYS = ["submitted", "completed", "failed", "pending", "inflight_batches", 
 
 
 class Server:
-    def __init__(self, budget_bytes=40 << 30, max_batch_clips=256, max_inflight=4):
+    def __init__(self, budget_bytes=40 << 30, max_batch_clips=256, max_inflight=4, host_pinned_bytes=0):
         cfg = ffi.new("MMServerConfig*")
         cfg.device_budget_bytes = int(budget_bytes)
         cfg.max_batch_clips = int(max_batch_clips)
         cfg.max_inflight = int(max_inflight)
+        cfg.host_pinned_bytes = int(host_pinned_bytes)
         st = ffi.new("int32_t*")
         self._borrowed = {}
         self._srv = lib.mm_server_create(cfg, st)

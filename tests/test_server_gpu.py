@@ -153,3 +153,17 @@ def test_borrowed_submits_equal_copied_submits():
     for x, y, z in zip(ra, rb, rc):
         np.testing.assert_array_equal(x, y)
         np.testing.assert_array_equal(x, z)
+
+
+def test_without_pinned_pool_room_results_are_unchanged():
+    """With a pinned pool too small for anything (1 MiB, below one pool
+    chunk), requests wait in pageable copies and batch results come back
+    through the slot's staging instead of pool blocks: the results are
+    bitwise those of a default server."""
+    reqs = _requests(10, seed=11)
+    with M.Server(max_inflight=2, max_batch_clips=4) as srv:
+        ref = [srv.result(i) for i in [srv.submit(y, **g) for y, g in reqs]]
+    with M.Server(max_inflight=2, max_batch_clips=4, host_pinned_bytes=1 << 20) as srv:
+        got = [srv.result(i) for i in [srv.submit(y, **g) for y, g in reqs]]
+    for x, y in zip(ref, got):
+        np.testing.assert_array_equal(x, y)

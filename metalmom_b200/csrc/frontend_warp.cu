@@ -183,7 +183,7 @@ struct WShape {
 };
 
 // Real-split twiddles W_N^(l + 32 i), i < 16, of lane l (one frame per warp
-// only): 512 complex, read as [32 i + l].
+// only): 512 complex, staged as pairs (i = 2p, 2p + 1) in float4 [32 p + l].
 template <int LOG2N>
 __host__ __device__ constexpr size_t warp_split_tw() {
   return WShape<LOG2N>::C == 1 ? size_t(16 * 32) * 8 : 0;
@@ -192,7 +192,7 @@ __host__ __device__ constexpr size_t warp_split_tw() {
 template <int LOG2N>
 __host__ __device__ constexpr size_t warp_fixed_smem() {
   using S = WShape<LOG2N>;
-  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + warp_split_tw<LOG2N>() +
+  return size_t(8) * S::TPF * 16 + align16(size_t(S::N) * 4) + warp_split_tw<LOG2N>() +
          size_t(S::F) * S::FSTRIDE * 8;
 }
 
@@ -250,18 +250,20 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   const bool lanes = a.mel_lane_ok != 0;
   const bool mel_in_smem = a.mel_nnz <= kMelSmemMax;
   unsigned char *sp = smem;
-  cpx *tw2 = reinterpret_cast<cpx *>(sp);  // W_M^(j k1), [k1-1][j]
-  sp += align16(size_t(31) * TPF * 8);
+  // stage-1 twiddles as pairs: tw4[p][j] = (W_M^(j (2p+1)), W_M^(j (2p+2))), p < 8
+  float4 *tw4 = reinterpret_cast<float4 *>(sp);
+  sp += size_t(8) * TPF * 16;
   float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
   sp += align16(size_t(N) * 4);
-  cpx *rs_tw = reinterpret_cast<cpx *>(sp);  // C == 1: real-split twiddles [32 i + l]
+  float4 *rs_tw = reinterpret_cast<float4 *>(sp);  // C == 1: real-split twiddle pairs [32 p + l]
   sp += warp_split_tw<LOG2N>();
   cpx *bufs = reinterpret_cast<cpx *>(sp);
   sp += size_t(F) * S::FSTRIDE * 8;
-  // lanes: band words, lane words, lane-minor weights; else packed rows
+  // lanes: band words, lane words, lane-minor weights (bins 2p, 2p + 1 of
+  // lane l as one float4 at [p][l], p < 17); else packed rows
   int *band_s = reinterpret_cast<int *>(sp);
   int2 *lane_s = reinterpret_cast<int2 *>(sp + align16(4 * (size_t)nmel));
-  float2 *lw_s = reinterpret_cast<float2 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);
+  float4 *lw_s = reinterpret_cast<float4 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);
   int4 *mel_s = reinterpret_cast<int4 *>(sp);
   float *melw_s = reinterpret_cast<float *>(sp + 16 * (size_t)nmel);
 
@@ -270,20 +272,30 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   const int l = lane - grp * TPF;   // lane within the frame group
   const float2 *twq = a.tw_split;   // W_N^t, t < N/4
 
-  for (int i = tid; i < 31 * TPF; i += S::THREADS) {
-    const int k1 = i / TPF + 1, j = i - (k1 - 1) * TPF;
-    tw2[i] = root_q(twq, 2 * j * k1, N);
+  for (int i = tid; i < 8 * TPF; i += S::THREADS) {
+    const int p = i / TPF, j = i - p * TPF;
+    const cpx u = root_q(twq, 2 * j * (2 * p + 1), N), w = root_q(twq, 2 * j * (2 * p + 2), N);
+    tw4[i] = make_float4(u.x, u.y, w.x, w.y);
   }
   for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the header comment
     const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
     reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
   }
   if constexpr (C == 1)
-    for (int i = tid; i < 16 * 32; i += S::THREADS) rs_tw[i] = root_q(twq, (i & 31) + 32 * (i >> 5), N);
+    for (int i = tid; i < 8 * 32; i += S::THREADS) {
+      const int p = i >> 5, ll = i & 31;
+      const cpx u = root_q(twq, ll + 64 * p, N), w = root_q(twq, ll + 32 * (2 * p + 1), N);
+      rs_tw[i] = make_float4(u.x, u.y, w.x, w.y);
+    }
   if (lanes) {
     for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
     for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
-    for (int i = tid; i < 33 * TPF; i += S::THREADS) lw_s[i] = __ldg(a.mel_lw + i);
+    for (int i = tid; i < 17 * TPF; i += S::THREADS) {
+      const int p = i / TPF, j = i - p * TPF;
+      const float2 u = __ldg(a.mel_lw + 2 * p * TPF + j);
+      const float2 w = 2 * p + 1 < 33 ? __ldg(a.mel_lw + (2 * p + 1) * TPF + j) : make_float2(0.0f, 0.0f);
+      lw_s[i] = make_float4(u.x, u.y, w.x, w.y);
+    }
   } else {
     for (int i = tid; i < nmel; i += S::THREADS) mel_s[i] = __ldg(a.mel_info + i);
     if (mel_in_smem)
@@ -385,13 +397,18 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       dft16(o);
       cpx *row = fb + l * 33;
       // W_M^(l (k + 16)) = W_M^(l k) W_M^(16 l): half of the table reads
-      const cpx g16 = tw2[15 * TPF + l];
+      const float4 t78 = tw4[7 * TPF + l];  // k = 15, 16
+      const cpx g16 = {t78.z, t78.w};
+      float4 tp = t78;
       static_for<0, 16>([&](auto ki) {
         constexpr int k = decltype(ki)::value;
         const cpx t = tw_const<k, 32>(o[k]);
         cpx lo = cadd(e[k], t), hi = csub(e[k], t);
         if constexpr (k > 0) {
-          const cpx tk = tw2[(k - 1) * TPF + l];
+          // pair k / 2 holds k (odd) and k + 1
+          if constexpr (k == 15) tp = t78;
+          else if constexpr (k % 2 == 1) tp = tw4[(k / 2) * TPF + l];
+          const cpx tk = (k % 2 == 1) ? cpx{tp.x, tp.y} : cpx{tp.z, tp.w};
           lo = cmul(lo, tk);
           hi = cmul(hi, cmul(tk, g16));
         } else {
@@ -427,6 +444,7 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       }
       const bool l0 = (l == 0);
       float *Pa = P + l;                              // bin l + 32 i at l + 33 i
+      float4 rsp;
       float *Pb = P + (M + TPF - 1 - l) + (l0 ? 1 : 0);  // bin M - l - 32 i, i > 0
       static_for<0, 16>([&](auto ki) {
         constexpr int i = decltype(ki)::value;
@@ -436,7 +454,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         else zb = l0 ? rcv[16 - i] : rcv[15 - i];
         const float ex = za.x + zb.x, ey = za.y - zb.y;
         const float ox = za.y + zb.y, oy = zb.x - za.x;
-        const cpx w = rs_tw[32 * i + l];  // W_N^(l + 32 i)
+        if constexpr (i % 2 == 0) rsp = rs_tw[32 * (i / 2) + l];
+        const cpx w = (i % 2 == 0) ? cpx{rsp.x, rsp.y} : cpx{rsp.z, rsp.w};  // W_N^(l + 32 i)
         const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
         const float xr = ex + wr, xi = ey + wi;
         const float yr = ex - wr, yi = ey - wi;
@@ -506,14 +525,16 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       const unsigned fl = (unsigned)li.x;
       int slot = li.y & 1023;
       const float *pl = P + 33 * l;
-      const float2 *wl = lw_s + l;
+      const float4 *wl = lw_s + l;
       // The frame's non-finite check: `tot` accumulates p * 0 over the lane's
       // bins (NaN for a NaN or inf bin, and no overflow), then a ballot.
       float R = 0.0f, Fs = 0.0f, tot = 0.0f;
+      float4 wq;
 #pragma unroll
       for (int b = 0; b < 32; b++) {
         const float p = pl[b];
-        const float2 w = wl[b * TPF];
+        if ((b & 1) == 0) wq = wl[(b >> 1) * TPF];
+        const float2 w = (b & 1) ? make_float2(wq.z, wq.w) : make_float2(wq.x, wq.y);
         tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
@@ -525,7 +546,8 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       }
       if (l == TPF - 1) {
         const float p = pl[32];
-        const float2 w = wl[32 * TPF];
+        const float4 wn = wl[16 * TPF];
+        const float2 w = make_float2(wn.x, wn.y);
         tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
@@ -1436,7 +1458,9 @@ static cudaError_t launch_warp2(const FrontArgs &a, int grid_limit, cudaStream_t
 template <int LOG2N>
 static cudaError_t launch_warp_t(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using S = WShape<LOG2N>;
-  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * 34 * (size_t)S::TPF
+  // lane walk: band words (4 n_mels, 16-aligned), lane words (8 TPF), weight
+  // pairs (17 x TPF float4); else the packed rows
+  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * (size_t)S::TPF + 16 * 17 * (size_t)S::TPF
                                       : mel_smem_bytes(a.n_mels, a.mel_nnz);
   const size_t smem = warp_fixed_smem<LOG2N>() + tables;
   auto kern = frame_warp_kernel<LOG2N>;

@@ -207,19 +207,20 @@ int warp_frames_per_tile(int log2n) {
   }
 }
 
-// Position of bin k in the padded power spectrum (k + min(k / 32, TPF - 1)).
-template <int TPF>
+// Position of bin k in the padded power spectrum: PS floats per 32 bins,
+// k + (PS - 32) min(k / 32, TPF - 1).
+template <int TPF, int PS = 33>
 __device__ __forceinline__ int pad_bin(int k) {
   const int q = k >> 5;
-  return k + (q < TPF - 1 ? q : TPF - 1);
+  return k + (PS - 32) * (q < TPF - 1 ? q : TPF - 1);
 }
 
 // mel_dot over the padded power spectrum.
-template <int TPF>
+template <int TPF, int PS = 33>
 __device__ __forceinline__ float mel_dot_pad(int4 info, const float *w, const float *P, bool bad) {
   const float *wr = w + info.z;
   float acc = 0.0f;
-  for (int q = 0; q < info.y; q++) acc = fmaf(wr[q], P[pad_bin<TPF>(info.x + q)], acc);
+  for (int q = 0; q < info.y; q++) acc = fmaf(wr[q], P[pad_bin<TPF, PS>(info.x + q)], acc);
   if (info.w || bad) acc = __int_as_float(0x7fc00000);
   return acc;
 }
@@ -242,6 +243,9 @@ template <int LOG2N>
 __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(FrontArgs a) {
   using S = WShape<LOG2N>;
   constexpr int N = S::N, M = S::M, TPF = S::TPF, C = S::C, HALF = S::HALF, F = S::F;
+  // floats per 32 bins of the padded power spectrum: 36 for one frame per
+  // warp, so that a lane's 32 bins are 16-byte aligned and read as float4
+  constexpr int PS = (TPF == 32) ? 36 : 33;
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char smem[];
   const int nmel = a.n_mels;
@@ -317,10 +321,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   }
 
   cpx *fb = bufs + (warp * S::FPW + grp) * S::FSTRIDE;
-  // power spectrum, padded: bin k at k + min(k / 32, TPF - 1), so that lane l
-  // of the group reads its bins [32 l, 32 l + 32) at 33 l + b, and the
-  // Nyquist bin M at 33 TPF - 1; group g starts TPF g floats into its buffer
-  // so that the groups of a warp fall in disjoint banks
+  // power spectrum, padded: bin k at k + (PS - 32) min(k / 32, TPF - 1), so
+  // that lane l of the group reads its bins [32 l, 32 l + 32) at PS l + b, and
+  // the Nyquist bin M at PS (TPF - 1) + 32; group g starts TPF g floats into
+  // its buffer so that the groups of a warp fall in disjoint banks
   float *P = reinterpret_cast<float *>(fb) + TPF * grp;
   const unsigned gmask = (TPF == 32) ? FULL : (((1u << TPF) - 1u) << (grp * TPF));
 
@@ -443,9 +447,11 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         rcv[m].y = __shfl_sync(FULL, v[16 + m].y, src);
       }
       const bool l0 = (l == 0);
-      float *Pa = P + l;                              // bin l + 32 i at l + 33 i
+      float *Pa = P + l;  // bin l + 32 i at l + PS i
       float4 rsp;
-      float *Pb = P + (M + TPF - 1 - l) + (l0 ? 1 : 0);  // bin M - l - 32 i, i > 0
+      // bin M - l - 32 i at M + (PS - 32)(TPF - 1) - l - PS i (lane 0, i > 0:
+      // PS - 32 further on; its i = 0 is the Nyquist bin)
+      float *Pb = P + (M + (PS - 32) * (TPF - 1) - l) + (l0 ? PS - 32 : 0);
       static_for<0, 16>([&](auto ki) {
         constexpr int i = decltype(ki)::value;
         const cpx za = v[i];
@@ -460,11 +466,11 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         const float xr = ex + wr, xi = ey + wi;
         const float yr = ex - wr, yi = ey - wi;
         const float p = fmaf(xr, xr, xi * xi), q = fmaf(yr, yr, yi * yi);
-        Pa[33 * i] = p;
-        if constexpr (i == 0) Pb[l0 ? -1 : 0] = q;  // lane 0: the Nyquist bin
-        else Pb[-33 * i] = q;
+        Pa[PS * i] = p;
+        if constexpr (i == 0) Pb[l0 ? -(PS - 32) : 0] = q;  // lane 0: the Nyquist bin
+        else Pb[-PS * i] = q;
       });
-      if (l0) P[M / 2 + TPF / 2] = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
+      if (l0) P[M / 2 + (PS - 32) * (TPF / 2)] = 4.0f * fmaf(rcv[0].x, rcv[0].x, rcv[0].y * rcv[0].y);
     } else {
       const bool l0 = (l == 0);
       static_for<0, HALF>([&](auto ci) {
@@ -520,19 +526,25 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       // every segment end; the lane holding a segment's head then adds the
       // parts of the lanes the segment runs into, and band m is the head of
       // segment m (.x) plus the head of segment m + 1 (.y).
-      float2 *parts = reinterpret_cast<float2 *>(P + 33 * TPF);
+      float2 *parts = reinterpret_cast<float2 *>(P + PS * TPF);
       const int2 li = lane_s[l];
       const unsigned fl = (unsigned)li.x;
       int slot = li.y & 1023;
-      const float *pl = P + 33 * l;
+      const float *pl = P + PS * l;
       const float4 *wl = lw_s + l;
       // The frame's non-finite check: `tot` accumulates p * 0 over the lane's
       // bins (NaN for a NaN or inf bin, and no overflow), then a ballot.
       float R = 0.0f, Fs = 0.0f, tot = 0.0f;
-      float4 wq;
+      float4 wq, pq;
 #pragma unroll
       for (int b = 0; b < 32; b++) {
-        const float p = pl[b];
+        float p;
+        if constexpr (PS % 4 == 0) {  // four bins per load
+          if ((b & 3) == 0) pq = reinterpret_cast<const float4 *>(pl)[b >> 2];
+          p = (b & 3) == 0 ? pq.x : (b & 3) == 1 ? pq.y : (b & 3) == 2 ? pq.z : pq.w;
+        } else {
+          p = pl[b];
+        }
         if ((b & 1) == 0) wq = wl[(b >> 1) * TPF];
         const float2 w = (b & 1) ? make_float2(wq.z, wq.w) : make_float2(wq.x, wq.y);
         tot = fmaf(p, 0.0f, tot);
@@ -581,10 +593,10 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
       }
     } else {
       float chk = 0.0f;  // the frame's non-finite check: this lane's share of the bins, times 0
-      for (int k = l; k <= M; k += TPF) chk = fmaf(P[pad_bin<TPF>(k)], 0.0f, chk);
+      for (int k = l; k <= M; k += TPF) chk = fmaf(P[pad_bin<TPF, PS>(k)], 0.0f, chk);
       const bool bad = (__ballot_sync(FULL, !isfinite(chk)) & gmask) != 0;
       for (int m = l; m < nmel; m += TPF) {
-        const float acc = mel_dot_pad<TPF>(mel_s[m], melw, P, bad);
+        const float acc = mel_dot_pad<TPF, PS>(mel_s[m], melw, P, bad);
         const float val = db10_frame(acc, a.amin, ref_db);
         if (valid) {
           dst[m] = val;

@@ -165,12 +165,17 @@ int warp_frames_per_tile(int log2n);  // 0 when the size has no warp kernel
 inline int mel_lane_tpf(int n_fft) {
   return (n_fft >= 256 && n_fft <= 4096 && (n_fft & (n_fft - 1)) == 0) ? n_fft / 64 : 0;
 }
-// Filterbank part slots that fit behind the padded spectrum (33 tpf floats):
-// in a warp-kernel frame buffer (66 tpf floats, frame group g starting tpf g
-// floats in) for tpf <= 32; 1024 (the slot field's range) for tpf = 64, whose
-// CTA-tile frame buffer holds more than 33 tpf + 2048 floats.
+// Filterbank part slots that fit behind the padded spectrum (ps tpf floats,
+// ps = 36 for tpf = 32 and 33 below): in a warp-kernel frame buffer (66 tpf
+// floats, frame group g starting tpf g floats in) for tpf <= 32 (480 at tpf
+// 32, also within the CTA-tile and tensor-core kernels' larger buffers); 1024
+// (the slot field's range) for tpf = 64, whose CTA-tile frame buffer holds
+// more than 33 tpf + 2048 floats.
 inline int mel_lane_max_slots(int tpf) {
-  return tpf <= 0 ? 0 : (tpf <= 32 ? (33 * tpf - tpf * (32 / tpf - 1)) / 2 : 1024);
+  if (tpf <= 0) return 0;
+  if (tpf > 32) return 1024;
+  const int ps = tpf == 32 ? 36 : 33;
+  return (66 * tpf - ps * tpf - tpf * (32 / tpf - 1)) / 2;
 }
 cudaError_t launch_frontend_tc(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched);
 cudaError_t launch_frontend_warp(int log2n, const FrontArgs &a, int grid_limit, cudaStream_t s,

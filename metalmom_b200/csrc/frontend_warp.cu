@@ -12,7 +12,8 @@
 //   k = k1 + 32 k2
 //   stage 1: 32-point DFT over r in registers       -> Y[j][k1]
 //            twiddle W_M^(j k1)
-//   one shared-memory transpose (row stride 33, conflict-free)
+//   one shared-memory transpose (row stride 33, conflict-free; one frame per
+//   warp: stored transposed with stride 34 and read back as float4)
 //   stage 2: TPF-point DFTs over j in registers      -> Z[k1 + 32 k2]
 //   real split X[k] = E + W_N^k O, X[M-k] = conj(E - W_N^k O), both from the
 //   pair (Z[k], Z[M-k]): the stage-2 columns are dealt to lanes so that k1
@@ -175,7 +176,9 @@ struct WShape {
   static constexpr int FPW = 32 / TPF;   // frames per warp
   static constexpr int C = FPW;          // stage-2 columns per lane
   static constexpr int HALF = C / 2;
-  static constexpr int FSTRIDE = TPF * 33;  // complex slots per frame buffer
+  // complex slots per frame buffer: TPF rows of 33 (one frame per warp: the
+  // stage-1 results stored transposed, 32 columns of 34)
+  static constexpr int FSTRIDE = TPF == 32 ? 32 * 34 : TPF * 33;
   static constexpr int NW = 8;              // warps per CTA
   static constexpr int THREADS = 32 * NW;
   static constexpr int F = NW * FPW;        // frames per CTA tile
@@ -257,7 +260,9 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
   // stage-1 twiddles as pairs: tw4[p][j] = (W_M^(j (2p+1)), W_M^(j (2p+2))), p < 8
   float4 *tw4 = reinterpret_cast<float4 *>(sp);
   sp += size_t(8) * TPF * 16;
-  float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
+  // analysis window (halved), the sample pairs of registers r, r + 1 of lane
+  // l as one float4 at [r / 2][l]
+  float4 *win_s = reinterpret_cast<float4 *>(sp);
   sp += align16(size_t(N) * 4);
   float4 *rs_tw = reinterpret_cast<float4 *>(sp);  // C == 1: real-split twiddle pairs [32 p + l]
   sp += warp_split_tw<LOG2N>();
@@ -281,9 +286,11 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     const cpx u = root_q(twq, 2 * j * (2 * p + 1), N), w = root_q(twq, 2 * j * (2 * p + 2), N);
     tw4[i] = make_float4(u.x, u.y, w.x, w.y);
   }
-  for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the header comment
-    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
-    reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
+  for (int i = tid; i < 16 * TPF; i += S::THREADS) {  // halved: see the header comment
+    const int p = i / TPF, j = i - p * TPF;
+    const float2 u = __ldg(reinterpret_cast<const float2 *>(a.window) + j + TPF * (2 * p));
+    const float2 w = __ldg(reinterpret_cast<const float2 *>(a.window) + j + TPF * (2 * p + 1));
+    win_s[i] = make_float4(0.5f * u.x, 0.5f * u.y, 0.5f * w.x, 0.5f * w.y);
   }
   if constexpr (C == 1)
     for (int i = tid; i < 8 * 32; i += S::THREADS) {
@@ -377,18 +384,22 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
     }
     // ---- window
     {
-      const float2 *wb = reinterpret_cast<const float2 *>(win_s) + l;
+      const float4 *wb = win_s + l;
 #pragma unroll
-      for (int r = 0; r < 32; r++) {
-        const float2 w = wb[TPF * r];
+      for (int r = 0; r < 32; r += 2) {
+        const float4 w = wb[TPF * (r / 2)];
         v[r].x *= w.x;
         v[r].y *= w.y;
+        v[r + 1].x *= w.z;
+        v[r + 1].y *= w.w;
       }
     }
 
     // ---- stage 1: 32-point DFT over registers; its last butterflies are
     // followed directly by the twiddle W_M^(l k1) and the store into row l of
-    // the frame buffer (stride 33), so that registers free up as it goes.
+    // the frame buffer (stride 33; one frame per warp: into column l of rows
+    // of 34, so that stage 2 reads its column as float4), so that registers
+    // free up as it goes.
     __syncwarp();  // the previous frame's mel reads of P are done
     {
       cpx e[16], o[16];
@@ -418,17 +429,32 @@ __global__ void __launch_bounds__(WShape<LOG2N>::THREADS, 2) frame_warp_kernel(F
         } else {
           hi = cmul(hi, g16);
         }
-        row[k] = lo;
-        row[k + 16] = hi;
+        if constexpr (C == 1) {
+          fb[k * 34 + l] = lo;
+          fb[(k + 16) * 34 + l] = hi;
+        } else {
+          row[k] = lo;
+          row[k + 16] = hi;
+        }
       });
     }
     __syncwarp();
-    static_for<0, C>([&](auto ci) {
-      constexpr int cc = decltype(ci)::value;
-      const int col = stage2_col<TPF, C, cc>(l);
+    if constexpr (C == 1) {  // column l: Y[jj][l] at 34 l + jj
+      const float4 *colp = reinterpret_cast<const float4 *>(fb + 34 * l);
 #pragma unroll
-      for (int jj = 0; jj < TPF; jj++) v[cc * TPF + jj] = fb[jj * 33 + col];
-    });
+      for (int jj = 0; jj < 32; jj += 2) {
+        const float4 y = colp[jj / 2];
+        v[jj] = {y.x, y.y};
+        v[jj + 1] = {y.z, y.w};
+      }
+    } else {
+      static_for<0, C>([&](auto ci) {
+        constexpr int cc = decltype(ci)::value;
+        const int col = stage2_col<TPF, C, cc>(l);
+#pragma unroll
+        for (int jj = 0; jj < TPF; jj++) v[cc * TPF + jj] = fb[jj * 33 + col];
+      });
+    }
     // ---- stage 2: TPF-point DFTs, v[c*TPF + k2] = Z[col(c) + 32 k2]
 #pragma unroll
     for (int cc = 0; cc < C; cc++) dft_any<TPF>(v + cc * TPF);

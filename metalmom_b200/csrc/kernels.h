@@ -166,9 +166,10 @@ inline int mel_lane_tpf(int n_fft) {
   return (n_fft >= 256 && n_fft <= 4096 && (n_fft & (n_fft - 1)) == 0) ? n_fft / 64 : 0;
 }
 // Filterbank part slots that fit behind the padded spectrum (ps tpf floats,
-// ps = 36 for tpf = 32 and 33 below): in a warp-kernel frame buffer (66 tpf
-// floats, frame group g starting tpf g floats in) for tpf <= 32 (480 at tpf
-// 32, also within the CTA-tile and tensor-core kernels' larger buffers); 1024
+// ps = 36 for tpf = 32 and 33 below): in a warp-kernel frame buffer (at
+// least 66 tpf floats, frame group g starting tpf g floats in) for tpf <= 32
+// (480 at tpf 32, also within the CTA-tile and tensor-core kernels' larger
+// buffers); 1024
 // (the slot field's range) for tpf = 64, whose CTA-tile frame buffer holds
 // more than 33 tpf + 2048 floats.
 inline int mel_lane_max_slots(int tpf) {

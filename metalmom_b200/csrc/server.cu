@@ -673,6 +673,7 @@ int32_t mm_server_poll(mm_server server, int64_t request_id, MMBuffer *out) {
     r = it->second;
     if (r->state == REQ_PENDING || r->state == REQ_RUNNING) return MM_PENDING;
     srv->reqs.erase(it);
+    srv->done_cv.notify_all();  // a waiter on this id learns it is gone
   }
   return deliver(srv, r, out);
 }
@@ -683,13 +684,21 @@ int32_t mm_server_wait(mm_server server, int64_t request_id, int32_t timeout_ms,
   Request *r = nullptr;
   {
     std::unique_lock<std::mutex> lk(srv->mu);
-    auto it = srv->reqs.find(request_id);
-    if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
-    r = it->second;
-    auto ready = [r] { return r->state == REQ_DONE || r->state == REQ_FAILED; };
+    if (srv->reqs.find(request_id) == srv->reqs.end()) return MM_ERR_INVALID_INPUT;
+    // looked up again on every wake-up: another caller may have taken the
+    // result (and deleted the request) meanwhile
+    auto ready = [&] {
+      auto it = srv->reqs.find(request_id);
+      if (it == srv->reqs.end()) return true;
+      return it->second->state == REQ_DONE || it->second->state == REQ_FAILED;
+    };
     if (timeout_ms < 0) srv->done_cv.wait(lk, ready);
     else if (!srv->done_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) return MM_PENDING;
-    srv->reqs.erase(request_id);
+    auto it = srv->reqs.find(request_id);
+    if (it == srv->reqs.end()) return MM_ERR_INVALID_INPUT;  // taken by another caller
+    r = it->second;
+    srv->reqs.erase(it);
+    srv->done_cv.notify_all();  // a second waiter on this id learns it is gone
   }
   return deliver(srv, r, out);
 }

@@ -167,3 +167,29 @@ def test_without_pinned_pool_room_results_are_unchanged():
         got = [srv.result(i) for i in [srv.submit(y, **g) for y, g in reqs]]
     for x, y in zip(ref, got):
         np.testing.assert_array_equal(x, y)
+
+
+def test_two_waiters_on_one_request():
+    """Two callers wait on the same request: one gets the result, the other
+    an invalid-request error (the request is gone once taken), and neither
+    waits on after the result is taken."""
+    y, g = _requests(1, seed=13)[0]
+    outcomes = []
+    with M.Server(max_inflight=1, max_batch_clips=1) as srv:
+        rid = srv.submit(y, **g)
+
+        def take():
+            try:
+                outcomes.append(("ok", srv.result(rid, timeout_ms=20000)))
+            except RuntimeError as e:
+                outcomes.append(("err", str(e)))
+
+        ts = [threading.Thread(target=take) for _ in range(2)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join(30)
+        assert not any(t.is_alive() for t in ts)
+    assert sorted(k for k, _ in outcomes) == ["err", "ok"]
+    res = next(v for k, v in outcomes if k == "ok")
+    assert O.mfcc_rel_error(res, _oracle(y, g)) < MFCC_TOL

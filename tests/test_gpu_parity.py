@@ -428,13 +428,13 @@ def test_plan_host_io_from_one_batch_array(length):
         np.testing.assert_array_equal(out[i], ref[i])
 
 
-@pytest.mark.parametrize("n_fft,hop,n_mels", [(2048, 512, 128), (512, 128, 120)])
+@pytest.mark.parametrize("n_fft,hop,n_mels", [(2048, 512, 128), (512, 128, 120), (2048, 512, 600)])
 def test_nonfinite_samples_floor_their_frames(n_fft, hop, n_mels):
     """A NaN or an infinite sample makes every band of the frames that hold it
     non-finite, which vDSP_vthr maps to amin (-100 dB) before the top_db floor;
     the other frames are untouched.  (2048, 128): the lane walk's check;
-    (512, 120): too many filterbank parts for the lane tables, so the packed
-    rows and their own check.)"""
+    (512, 120) and (2048, 600): too many filterbank parts for the lane tables,
+    so the packed rows and their own check.)"""
     y = synth.music_clip(22050, SR, seed=31)
     y[5000] = np.nan
     y[15000] = np.inf
@@ -451,6 +451,8 @@ def test_nonfinite_samples_floor_their_frames(n_fft, hop, n_mels):
     (2048, 20, 0.0, None),       # wide bands: segments over several lanes
     (2048, 64, 300.0, 4000.0),   # bins past fmax carry the last segment to the end
     (2048, 256, 0.0, None),
+    (2048, 400, 0.0, None),      # 32 walking lanes: under their 480 part slots
+    (2048, 600, 0.0, None),      # over them: packed rows over the 36-float padded spectrum
     (1024, 64, 0.0, None),
     (512, 100, 0.0, None),       # lane tables near their slot limit
     (512, 120, 0.0, None),       # over it: packed rows

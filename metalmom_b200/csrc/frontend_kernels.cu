@@ -1517,7 +1517,8 @@ __global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
   }
 }
 
-// 128 bands: the DCT-II basis is symmetric in n for even k and antisymmetric
+// NM bands (64, 80 or 128: a multiple of 16, so a half row is an even number
+// of float4 chunks): the DCT-II basis is symmetric in n for even k and antisymmetric
 // for odd k (cos(pi k (2(N-1-n)+1) / 2N) = (-1)^k cos(pi k (2n+1) / 2N)), so
 // with e_n = x_n + x_{N-1-n} and o_n = x_n - x_{N-1-n} (n < N/2) the even
 // coefficients are sum_n B[k][n] e_n and the odd ones sum_n B[k][n] o_n: half
@@ -1529,20 +1530,23 @@ __global__ void __launch_bounds__(256, 2) dct_pipe_kernel(DctArgs a) {
 // - a tile's rows are copied straight into shared memory by cp.async (no
 //   registers in flight), two tile buffers, the next tile's copies issued
 //   before this one is folded;
-// - the floor and the even/odd fold run in place in shared memory: a thread
-//   takes float4 chunks j, 15 - j of a row and their mirrors 31 - j, 16 + j,
-//   reads all four, then writes e over chunks j, 15 - j and o over 16 + j,
-//   31 - j (the row becomes [e | o]);
+// - the floor and the even/odd fold run in place in shared memory: with C4 =
+//   NM / 4 chunks a row and H4 = C4 / 2, a thread takes float4 chunks j,
+//   H4 - 1 - j of a row and their mirrors C4 - 1 - j, H4 + j, reads all four,
+//   then writes e over chunks j, H4 - 1 - j and o over H4 + j, C4 - 1 - j
+//   (the row becomes [e | o]);
 // - 128 threads, each two frames (lane, lane + 32) x KQ coefficients of its
 //   warp's group, so every basis read from shared memory feeds two frames.
-constexpr int kDct2Stride = 132;  // floats per staged row (16-byte aligned, conflict-free reads)
+// floats per staged row: NM + 4 mod 32 (16-byte aligned; a warp's 32 row reads conflict-free)
+__host__ __device__ constexpr int dct2_stride(int nm) { return nm + ((36 - (nm & 31)) & 31); }
 // Tile buffers in the copy ring: two (3 CTAs per SM) measured 0.0618 ms per
 // bench step against 0.0677 ms for three (2 CTAs per SM).
 constexpr int kDctFoldStages = 2;
 
-template <int KQ, int S>
+template <int KQ, int S, int NM>
 __global__ void __launch_bounds__(128, S == 2 ? 3 : 2) dct_fold2_kernel(DctArgs a) {
-  constexpr int NM = 128, H = NM / 2, H4 = H / 4, TS = kDct2Stride;
+  static_assert(NM % 16 == 0 && NM <= 128, "a half row must be an even number of float4 chunks");
+  constexpr int H = NM / 2, H4 = H / 4, C4 = NM / 4, TS = dct2_stride(NM);
   extern __shared__ __align__(16) float dsm[];
   float *buf0 = dsm;                     // [kDctTile][TS] x S
   float *bas = dsm + S * kDctTile * TS;  // [4*KQ][H]
@@ -1569,12 +1573,13 @@ __global__ void __launch_bounds__(128, S == 2 ? 3 : 2) dct_fold2_kernel(DctArgs 
     m.T = cd.n_frames;
     return m;
   };
-  // rows r < nt of tile m into buffer b: chunk i = tid + 128 u is row i / 32, float4 i % 32
+  // rows r < nt of tile m into buffer b: chunk i = tid + 128 u is row i / C4, float4 i % C4
   auto issue = [&](const DctTileMeta &m, float *b) {
+    static_assert(kDctTile * C4 % 128 == 0, "whole copy rounds");
 #pragma unroll
-    for (int u = 0; u < kDctTile * 32 / 128; u++) {
-      const int i = tid + 128 * u, r = i >> 5, c4 = i & 31;
-      if (r < m.nt) cp_async16(b + r * TS + 4 * c4, m.src + r * 32 + c4);
+    for (int u = 0; u < kDctTile * C4 / 128; u++) {
+      const int i = tid + 128 * u, r = i / C4, c4 = i - r * C4;
+      if (r < m.nt) cp_async16(b + r * TS + 4 * c4, m.src + r * C4 + c4);
     }
     cp_async_commit();
   };
@@ -1611,22 +1616,22 @@ __global__ void __launch_bounds__(128, S == 2 ? 3 : 2) dct_fold2_kernel(DctArgs 
       f2 = __ldg(a.tile_first + t2);
     }
     __syncthreads();  // every thread's copies of this tile have landed
-    // floor + fold in place: unit i = tid + 128 u is row i / 8, chunk pair j = i % 8
+    // floor + fold in place: unit i is row i / (H4 / 2), chunk pair j = i % (H4 / 2)
 #pragma unroll
-    for (int u = 0; u < kDctTile * 8 / 128; u++) {
-      const int i = tid + 128 * u, r = i >> 3, j = i & 7;
+    for (int i = tid; i < kDctTile * (H4 / 2); i += 128) {
+      const int r = i / (H4 / 2), j = i - r * (H4 / 2);
       if (r < cur.nt) {
         float4 *row = reinterpret_cast<float4 *>(b + r * TS);
-        float4 A = row[j], Am = row[31 - j], B = row[15 - j], Bm = row[16 + j];
+        float4 A = row[j], Am = row[C4 - 1 - j], B = row[H4 - 1 - j], Bm = row[H4 + j];
         const float t = cur.thr;
         A = make_float4(vthr(A.x, t), vthr(A.y, t), vthr(A.z, t), vthr(A.w, t));
         Am = make_float4(vthr(Am.x, t), vthr(Am.y, t), vthr(Am.z, t), vthr(Am.w, t));
         B = make_float4(vthr(B.x, t), vthr(B.y, t), vthr(B.z, t), vthr(B.w, t));
         Bm = make_float4(vthr(Bm.x, t), vthr(Bm.y, t), vthr(Bm.z, t), vthr(Bm.w, t));
         row[j] = make_float4(A.x + Am.w, A.y + Am.z, A.z + Am.y, A.w + Am.x);
-        row[16 + j] = make_float4(A.x - Am.w, A.y - Am.z, A.z - Am.y, A.w - Am.x);
-        row[15 - j] = make_float4(B.x + Bm.w, B.y + Bm.z, B.z + Bm.y, B.w + Bm.x);
-        row[31 - j] = make_float4(B.x - Bm.w, B.y - Bm.z, B.z - Bm.y, B.w - Bm.x);
+        row[H4 + j] = make_float4(A.x - Am.w, A.y - Am.z, A.z - Am.y, A.w - Am.x);
+        row[H4 - 1 - j] = make_float4(B.x + Bm.w, B.y + Bm.z, B.z + Bm.y, B.w + Bm.x);
+        row[C4 - 1 - j] = make_float4(B.x - Bm.w, B.y - Bm.z, B.z - Bm.y, B.w - Bm.x);
       }
     }
     // its clip's words
@@ -1674,22 +1679,27 @@ __global__ void __launch_bounds__(128, S == 2 ? 3 : 2) dct_fold2_kernel(DctArgs 
   }
 }
 
-template <int KQ, int S>
+template <int KQ, int S, int NM>
 static cudaError_t launch_dct_fold2_s(const DctArgs &a, cudaStream_t s) {
-  const size_t smem = sizeof(float) * ((size_t)S * kDctTile * kDct2Stride + (size_t)4 * KQ * 64);
+  const size_t smem = sizeof(float) * ((size_t)S * kDctTile * dct2_stride(NM) + (size_t)4 * KQ * (NM / 2));
   int per_sm = 1, sms = 148;
   cudaError_t e =
-      persistent_geometry(reinterpret_cast<const void *>(dct_fold2_kernel<KQ, S>), 128, smem, &per_sm, &sms);
+      persistent_geometry(reinterpret_cast<const void *>(dct_fold2_kernel<KQ, S, NM>), 128, smem, &per_sm, &sms);
   if (e != cudaSuccess) return e;
   long long grid = (long long)sms * per_sm;
   if (grid > a.total_tiles) grid = a.total_tiles;
-  dct_fold2_kernel<KQ, S><<<(unsigned)grid, 128, smem, s>>>(a);
+  dct_fold2_kernel<KQ, S, NM><<<(unsigned)grid, 128, smem, s>>>(a);
   return cudaGetLastError();
 }
 
+// n_mels 64, 80 or 128 (the bands of the default, speech and mixed-batch front ends)
 template <int KQ>
 static cudaError_t launch_dct_fold2_t(const DctArgs &a, cudaStream_t s) {
-  return launch_dct_fold2_s<KQ, kDctFoldStages>(a, s);
+  switch (a.n_mels) {
+    case 64: return launch_dct_fold2_s<KQ, kDctFoldStages, 64>(a, s);
+    case 80: return launch_dct_fold2_s<KQ, kDctFoldStages, 80>(a, s);
+    default: return launch_dct_fold2_s<KQ, kDctFoldStages, 128>(a, s);
+  }
 }
 
 template <int KQ>
@@ -1731,7 +1741,7 @@ cudaError_t launch_dct(const DctArgs &a, cudaStream_t s) {
   if (a.total_tiles <= 0 || a.n_mfcc <= 0) return cudaSuccess;
   // 4 coefficient groups x KQ accumulators cover min(n_mfcc, 32) coefficients per pass
   const int kq = (std::min(a.n_mfcc, kDctKC) + 3) / 4;
-  if (a.n_mfcc <= kDctKC && a.n_mels == 128) {
+  if (a.n_mfcc <= kDctKC && (a.n_mels == 128 || a.n_mels == 80 || a.n_mels == 64)) {
     switch ((a.n_mfcc + 3) / 4) {  // ceil(ceil(n_mfcc / 2) / 2)
       case 1: return launch_dct_fold2_t<1>(a, s);
       case 2: return launch_dct_fold2_t<2>(a, s);

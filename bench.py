@@ -440,26 +440,49 @@ def serving_leg(duration=3.0, rates=(50, 500, 2000), burst=2000, plain_s=2.0, n_
     return res
 
 
-def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
-    """The uneven batch: 1024 clips, lengths uniform in 1-120 s, each clip
-    with its own group (sr 22050/44100, n_fft 1024/2048/4096 with hop n_fft/4,
-    64/128 mels, 20 MFCC); launch variants autotuned per n_fft; one grouped
-    plan (a graph of concurrent persistent launches, one branch per group),
-    inputs resident, CUDA events around `steps` graph replays."""
-    import torch
-    import metalmom_b200 as M
-    from metalmom_b200 import synth
+def uneven_workload(n_clips=1024, seed=2024):
+    """The uneven batch's clips without their audio: per clip (group params,
+    start offset, samples), drawn from one seeded generator, the same on
+    every rank."""
     rng = np.random.default_rng(seed)
-    pools = {sr: synth.music_clip(120 * sr, sr, seed=sr) for sr in (22050, 44100)}
-    params, clips = [], []
+    work = []
     for _ in range(n_clips):
         n_fft = int(rng.choice([1024, 2048, 4096]))
         g = dict(sr=int(rng.choice([22050, 44100])), n_fft=n_fft, hop_length=n_fft // 4,
                  n_mels=int(rng.choice([64, 128])), n_mfcc=20)
         n = int(rng.uniform(1.0, 120.0) * g["sr"])
-        start = int(rng.integers(0, len(pools[g["sr"]]) - n + 1))
-        params.append(g)
-        clips.append(pools[g["sr"]][start:start + n])
+        start = int(rng.integers(0, 120 * g["sr"] - n + 1))
+        work.append((g, start, n))
+    return work
+
+
+def uneven_shard(work, rank, world):
+    """This rank's clip indices: `balanced_shards` over the clips' device cost
+    (frames x per-frame cost of their group), in workload order."""
+    from metalmom_b200.shard import balanced_shards
+    shards = balanced_shards([n for _, _, n in work], world, [g for g, _, _ in work])
+    return sorted(shards[rank])
+
+
+def uneven_leg(stream, rank=0, world=1, dist=None, steps=20, n_clips=1024, seed=2024):
+    """The uneven batch: 1024 clips, lengths uniform in 1-120 s, each clip
+    with its own group (sr 22050/44100, n_fft 1024/2048/4096 with hop n_fft/4,
+    64/128 mels, 20 MFCC); launch variants autotuned per n_fft; one grouped
+    plan (a graph of concurrent persistent launches, one branch per group),
+    inputs resident, CUDA events around `steps` graph replays.  With several
+    ranks the clips are routed by device cost (`uneven_shard`), each rank
+    runs its own plan, and the time is the max over ranks."""
+    import torch
+    import metalmom_b200 as M
+    from metalmom_b200 import synth
+    from metalmom_b200.shard import clip_cost, frames_of, max_over_ranks
+    pools = {sr: synth.music_clip(120 * sr, sr, seed=sr) for sr in (22050, 44100)}
+    work = uneven_workload(n_clips, seed)
+    mine = uneven_shard(work, rank, world)
+    all_hours = sum(n / g["sr"] for g, _, n in work) / 3600.0
+    costs = [sum(clip_cost(work[i][2], **work[i][0]) for i in uneven_shard(work, r, world)) for r in range(world)]
+    params = [work[i][0] for i in mine]
+    clips = [pools[work[i][0]["sr"]][work[i][1]:work[i][1] + work[i][2]] for i in mine]
     tuned = {}
     for n_fft in (1024, 2048, 4096):
         tuned[n_fft] = M.autotune(clip_samples=30 * 22050, n_clips=32, reps=3, sr=22050, n_fft=n_fft,
@@ -470,14 +493,20 @@ def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
     for _ in range(3):
         plan.execute(stream=sh)
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
     for _ in range(steps):
         plan.execute(stream=sh)
     b.record(stream)
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / steps
-    hours = sum(len(c) / g["sr"] for c, g in zip(clips, params)) / 3600.0
+    ms = max_over_ranks(a.elapsed_time(b) / steps, dist, device="cuda")
+    if rank != 0:
+        plan.close()
+        return None
+    hours = all_hours
     # the longest clip of every group: its MFCC and log-mel rows from the last
     # replay against the FP64 oracle
     res = plan.execute_host(clips, stream=sh)
@@ -495,12 +524,16 @@ def uneven_leg(stream, steps=20, n_clips=1024, seed=2024):
     out = {"workload": f"{n_clips} clips, lengths U[1,120] s, per-clip group from sr {{22050, 44100}} x "
                        "n_fft {1024, 2048, 4096} (hop n_fft/4) x mels {64, 128}, 20 MFCC",
            "audio_hours": hours, "ms_per_step": ms, "audio_hours_per_s": hours / (ms / 1e3),
-           "samples_per_s": sum(len(c) for c in clips) / (ms / 1e3),
-           "frames_per_s": sum(plan.frames) / (ms / 1e3),
+           "samples_per_s": sum(n for _, _, n in work) / (ms / 1e3),
+           "frames_per_s": sum(frames_of(n, g["n_fft"], g["hop_length"], True) for g, _, n in work) / (ms / 1e3),
+           "sharding": ("1 GPU" if world == 1 else
+                        f"{world} ranks, clips routed by device cost (balanced_shards), max over ranks; "
+                        f"rank cost max / mean {max(costs) / (sum(costs) / world):.3f}"),
            "groups": len({tuple(sorted(g.items())) for g in params}), "branches": plan.branches,
            "gpu_launches_per_step": plan.kernel_launches, "tuned_variant_per_n_fft": tuned,
            "timing": "CUDA events around graph replays, inputs resident (> L2)",
-           "accuracy": merge_errors(errs, "the longest clip of each group")}
+           "accuracy": merge_errors(errs, "the longest clip of each group" +
+                                    ("" if world == 1 else " among rank 0's clips"))}
     plan.close()
     return out
 
@@ -651,6 +684,9 @@ def run_ours(args, rank, world, local_rank):
     d2h = sum(o.nbytes for o in out_np)
     copy = copy_probe(h2d, d2h, stream, in_np[0].nbytes) if rank == 0 else None
 
+    # ---- the uneven mixed-group batch: every rank, clips routed by device cost
+    uneven = None if args.no_uneven else uneven_leg(stream, rank, world, dist)
+
     # ---- the plain one-clip-per-launch GPU form, for comparison
     per_clip = None
     if rank == 0:
@@ -747,8 +783,8 @@ def run_ours(args, rank, world, local_rank):
             result.update(baseline_leg(plan, clips, world, args))
         if not args.no_serve:
             result["serving"] = serving_leg()
-        if not args.no_uneven:
-            result["uneven_batch"] = uneven_leg(stream)
+        if uneven is not None:
+            result["uneven_batch"] = uneven
         if not args.no_precision:
             result["precision_forms"] = precision_leg(stream)
         # per-leg accuracy against the FP64 oracle, in one place

@@ -62,3 +62,17 @@ def test_router_sends_requests_to_the_least_loaded_device():
         for h in short:
             r.result(h)
         assert all(v == 0.0 for v in r.load)
+
+
+def test_bench_uneven_batch_routed_over_ranks():
+    """The bench's uneven mixed-group batch at N GPUs: every clip goes to
+    exactly one rank, the ranks' device costs are within 1 % of each other,
+    and one rank keeps the whole batch in workload order."""
+    import bench
+    work = bench.uneven_workload()
+    assert bench.uneven_shard(work, 0, 1) == list(range(len(work)))
+    for world in (2, 4, 8):
+        shards = [bench.uneven_shard(work, r, world) for r in range(world)]
+        assert sorted(i for s in shards for i in s) == list(range(len(work)))
+        costs = [sum(clip_cost(work[i][2], **work[i][0]) for i in s) for s in shards]
+        assert max(costs) <= 1.01 * (sum(costs) / world)

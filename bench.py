@@ -208,8 +208,11 @@ def _device_floats(ptr, n):
 def oracle_errors(y, g, mfcc_out, mel_rows=None, clip_max_db=None):
     """Errors of one clip's result against the FP64 oracle: MFCC as max |err|
     / max |c|, and (given the clip's frame-major log-mel rows and maximum)
-    mel-dB after the top_db floor, overall and within 60 dB of the maximum."""
-    from oracle import oracle as O
+    mel-dB after the top_db floor, overall, within 60 dB of the maximum, and
+    60-80 dB below it beside the reference's own float32 path (the C port)
+    on the same values: the bar there is max(1e-3 dB, 2 x the reference's
+    error), as in the GPU tests."""
+    from oracle import oracle as O, refcpu
     sr, n_fft = g["sr"], g["n_fft"]
     hop, win = g.get("hop_length") or n_fft // 4, g.get("win_length") or n_fft
     n_mels, n_mfcc = g.get("n_mels", 128), g.get("n_mfcc", 20)
@@ -223,6 +226,13 @@ def oracle_errors(y, g, mfcc_out, mel_rows=None, clip_max_db=None):
         near = exp_db >= exp_db.max() - 60.0
         out["mel_db"] = float(err.max())
         out["mel_db_within_60db"] = float(err[near].max())
+        far = ~near
+        if far.any():
+            _, ref_db = refcpu.mfcc(y, sr, n_mfcc, n_fft, hop, win, n_mels, g.get("fmin", 0.0),
+                                    g.get("fmax") or 0.0, True, want_mel_db=True)
+            err_ref = np.abs(np.asarray(ref_db, np.float64) - exp_db)
+            out["mel_db_60_80db"] = float(err[far].max())
+            out["reference_f32_mel_db_60_80db"] = float(err_ref[far].max())
     return out
 
 
@@ -233,6 +243,14 @@ def merge_errors(errs, what):
     if any("mel_db" in e for e in errs):
         out["mel_db_max_abs_err_db"] = max(e["mel_db"] for e in errs if "mel_db" in e)
         out["mel_db_max_abs_err_db_within_60db"] = max(e["mel_db_within_60db"] for e in errs if "mel_db" in e)
+    far = [e for e in errs if "mel_db_60_80db" in e]
+    if far:
+        out["mel_db_60_80db"] = {
+            "max_abs_err_db": max(e["mel_db_60_80db"] for e in far),
+            "reference_f32_max_abs_err_db": max(e["reference_f32_mel_db_60_80db"] for e in far),
+            "within_bar": all(e["mel_db_60_80db"] <= max(1e-3, 2.0 * e["reference_f32_mel_db_60_80db"])
+                              for e in far),
+            "bar": "per clip: max(1e-3 dB, 2 x the reference float32 path's error on the same values)"}
     return out
 
 

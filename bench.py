@@ -482,14 +482,16 @@ def uneven_shard(work, rank, world):
     return sorted(shards[rank])
 
 
-def uneven_leg(stream, rank=0, world=1, dist=None, steps=20, n_clips=1024, seed=2024):
+def uneven_leg(stream, rank=0, world=1, dist=None, steps=20, n_clips=1024, seed=2024, variant=None):
     """The uneven batch: 1024 clips, lengths uniform in 1-120 s, each clip
     with its own group (sr 22050/44100, n_fft 1024/2048/4096 with hop n_fft/4,
     64/128 mels, 20 MFCC); launch variants autotuned per n_fft; one grouped
     plan (a graph of concurrent persistent launches, one branch per group),
     inputs resident, CUDA events around `steps` graph replays.  With several
     ranks the clips are routed by device cost (`uneven_shard`), each rank
-    runs its own plan, and the time is the max over ranks."""
+    runs its own plan, and the time is the max over ranks.  `variant`: one
+    fixed launch variant for every n_fft instead of the autotuner (profiling
+    runs, where the tuner's timings are distorted)."""
     import torch
     import metalmom_b200 as M
     from metalmom_b200 import synth
@@ -503,8 +505,12 @@ def uneven_leg(stream, rank=0, world=1, dist=None, steps=20, n_clips=1024, seed=
     clips = [pools[work[i][0]["sr"]][work[i][1]:work[i][1] + work[i][2]] for i in mine]
     tuned = {}
     for n_fft in (1024, 2048, 4096):
-        tuned[n_fft] = M.autotune(clip_samples=30 * 22050, n_clips=32, reps=3, sr=22050, n_fft=n_fft,
-                                  hop_length=n_fft // 4, n_mels=128, n_mfcc=20)["best"]
+        if variant is not None:
+            M.tune_set(n_fft, variant)
+            tuned[n_fft] = variant
+        else:
+            tuned[n_fft] = M.autotune(clip_samples=30 * 22050, n_clips=32, reps=3, sr=22050, n_fft=n_fft,
+                                      hop_length=n_fft // 4, n_mels=128, n_mfcc=20)["best"]
     plan = M.Plan([len(c) for c in clips], clip_params=params)
     sh = stream.cuda_stream
     plan.execute_host(clips, stream=sh)
@@ -703,7 +709,7 @@ def run_ours(args, rank, world, local_rank):
     copy = copy_probe(h2d, d2h, stream, in_np[0].nbytes) if rank == 0 else None
 
     # ---- the uneven mixed-group batch: every rank, clips routed by device cost
-    uneven = None if args.no_uneven else uneven_leg(stream, rank, world, dist)
+    uneven = None if args.no_uneven else uneven_leg(stream, rank, world, dist, variant=args.variant)
 
     # ---- the plain one-clip-per-launch GPU form, for comparison
     per_clip = None
@@ -906,7 +912,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-uneven", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
-    ap.add_argument("--variant", type=int, default=None, help="fixed frame-kernel launch variant (no autotuning)")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="fixed frame-kernel launch variant for every n_fft (no autotuning)")
     ap.add_argument("--e2e-branch-clips", type=int, default=32)
     ap.add_argument("--kernel-case", type=int, default=None, metavar="N_FFT",
                     help="only a device-resident plan at this n_fft (kernel profiles); no bench line")

@@ -151,6 +151,23 @@ CPU_PORTS = {
 }
 
 
+def steady_allocator():
+    """glibc malloc in the state a long-running process reaches by itself
+    after its first large frees: blocks up to 32 MB from the heap and freed
+    memory kept.  A fresh process otherwise maps and unmaps the CPU ports'
+    per-clip arrays on every call and spends about half of its time in page
+    faults (measured on the B200 hosts' 16 cores: 3.5 audio-h/s for the NumPy
+    port in a fresh process against 6.4 in a warm one).  True when set."""
+    import ctypes
+    try:
+        libc = ctypes.CDLL("libc.so.6")
+    except OSError:
+        return False
+    M_TRIM_THRESHOLD, M_MMAP_THRESHOLD = -1, -3
+    ok = libc.mallopt(M_MMAP_THRESHOLD, 32 << 20) == 1
+    return bool(libc.mallopt(M_TRIM_THRESHOLD, 1 << 30) == 1 and ok)
+
+
 def cpu_port(name):
     """The MFCC-of-a-clip-list function of one CPU port, all host threads."""
     if name == "refcpu":
@@ -181,13 +198,14 @@ def cpu_baseline(clips, n_sample):
     the faster one is the reported baseline."""
     sample = clips[:n_sample]
     threads = os.cpu_count() or 1
+    steady = steady_allocator()
     secs = time_cpu_ports(sample)
     hours = len(sample) * CLIP_SAMPLES / SR / 3600.0
     best = next(iter(secs))
     return {"value": hours / secs[best], "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{len(sample)} of the {len(clips)} clips (30 s each); the faster of two CPU ports: "
                       f"{best} ({CPU_PORTS[best]})",
-            "seconds": secs[best],
+            "seconds": secs[best], "allocator": "steady (mallopt)" if steady else "default",
             "ports": {k: {"audio_hours_per_s": hours / v, "seconds": v, "what": CPU_PORTS[k]}
                       for k, v in secs.items()}}
 
@@ -840,6 +858,7 @@ def run_reference(args, rank):
     threads = os.cpu_count() or 1
     n = args.ref_clips
     clips = make_clips(n, seed0=0)
+    steady = steady_allocator()
     secs = time_cpu_ports(clips)  # picks the port; not part of the timed steps
     port = next(iter(secs))
     fn = cpu_port(port)
@@ -861,7 +880,8 @@ def run_reference(args, rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(N_CLIPS), "impl": "reference",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample,
-                         "ports_one_step_s": secs},
+                         "ports_one_step_s": secs,
+                         "allocator": "steady (mallopt)" if steady else "default"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "MetalMom's CPU path is Swift + Apple Accelerate and cannot be built on Linux; this arm times "
                 "the faster of its two CPU stand-ins (oracle/refcpu.c, oracle/librosa_port.py) on the host cores.",

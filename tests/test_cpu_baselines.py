@@ -39,3 +39,11 @@ def test_refcpu_matches_oracle():
         e = O.mel_db(y, 22050, 2048, 512, 2048, True, 128)
         near = e >= e.max() - 60.0
         assert np.abs(d - e)[near].max() < 1e-3
+
+
+def test_steady_allocator_applies():
+    """The bench times the CPU ports with glibc malloc at its steady state
+    (large blocks from the heap, freed memory kept); the setting takes on
+    this C library."""
+    import bench
+    assert bench.steady_allocator() is True

@@ -670,7 +670,7 @@ struct W2Shape {
 
 __host__ __device__ constexpr size_t warp2_fixed_smem() {
   using S = W2Shape;
-  return align16(size_t(31) * S::TPF * 8) + align16(size_t(S::N) * 4) + align16(size_t(S::RS) * 8) +
+  return size_t(8) * S::TPF * 16 + align16(size_t(S::N) * 4) + align16(size_t(S::RS) * 8) +
          size_t(S::F) * S::FSTRIDE * 8;
 }
 
@@ -684,11 +684,17 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
   const bool lanes = a.mel_lane_ok != 0;
   const bool mel_in_smem = a.mel_nnz <= S::MEL_SMEM_MAX;
   unsigned char *sp = smem;
-  cpx *tw2 = reinterpret_cast<cpx *>(sp);  // W_M^(j k1), [k1-1][j]
-  sp += align16(size_t(31) * TPF * 8);
-  float *win_s = reinterpret_cast<float *>(sp);  // analysis window, natural order
+  // The tables a thread reads once per frame are staged as float4 pairs of
+  // the entries it reads in turn (half the load instructions, same bytes):
+  // stage-1 twiddles tw4[p][j] = (W_M^(j (2p+1)), W_M^(j (2p+2))), p < 8
+  float4 *tw4 = reinterpret_cast<float4 *>(sp);
+  sp += size_t(8) * TPF * 16;
+  // the halved window: samples of registers r, r + 1 of thread j at [r / 2][j]
+  float4 *win_s = reinterpret_cast<float4 *>(sp);
   sp += align16(size_t(N) * 4);
-  cpx *rs_tw = reinterpret_cast<cpx *>(sp);  // W_N^(c + 32 s) at 33 s + c
+  // real-split twiddles: row 2p + j0, column c holds (W_N^(c + 32 (4p + j0)),
+  // W_N^(c + 32 (4p + 2 + j0))), rows of 33 (conflict-free)
+  float4 *rs_tw = reinterpret_cast<float4 *>(sp);
   sp += align16(size_t(S::RS) * 8);
   cpx *bufs = reinterpret_cast<cpx *>(sp);
   sp += size_t(F) * S::FSTRIDE * 8;
@@ -696,7 +702,7 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
   // (the packed rows' descriptors are read from global memory)
   int *band_s = reinterpret_cast<int *>(sp);
   int2 *lane_s = reinterpret_cast<int2 *>(sp + align16(4 * (size_t)nmel));
-  float2 *lw_s = reinterpret_cast<float2 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);
+  float4 *lw_s = reinterpret_cast<float4 *>(sp + align16(4 * (size_t)nmel) + 8 * TPF);  // weight pairs [p][j]
   float *melw_s = reinterpret_cast<float *>(sp);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -709,22 +715,35 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
   const int partner = 2 * (half ? 15 - (lane >> 1) : (16 - (lane >> 1)) & 15) + (1 - j0);
   const float2 *twq = a.tw_split;  // W_N^t, t < N/4
 
-  for (int i = tid; i < 31 * TPF; i += S::THREADS) {
-    const int k1 = i / TPF + 1, jj = i - (k1 - 1) * TPF;
-    tw2[i] = root_q(twq, 2 * jj * k1, N);
+  for (int i = tid; i < 8 * TPF; i += S::THREADS) {
+    const int p = i / TPF, jj = i - p * TPF;
+    const cpx u = root_q(twq, 2 * jj * (2 * p + 1), N), w = root_q(twq, 2 * jj * (2 * p + 2), N);
+    tw4[i] = make_float4(u.x, u.y, w.x, w.y);
   }
-  for (int i = tid; i < N / 4; i += S::THREADS) {  // halved: see the header comment
-    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.window) + i);
-    reinterpret_cast<float4 *>(win_s)[i] = make_float4(0.5f * w.x, 0.5f * w.y, 0.5f * w.z, 0.5f * w.w);
+  for (int i = tid; i < 16 * TPF; i += S::THREADS) {  // halved: see the header comment
+    const int p = i / TPF, jj = i - p * TPF;
+    const float2 u = __ldg(reinterpret_cast<const float2 *>(a.window) + jj + TPF * (2 * p));
+    const float2 w = __ldg(reinterpret_cast<const float2 *>(a.window) + jj + TPF * (2 * p + 1));
+    win_s[i] = make_float4(0.5f * u.x, 0.5f * u.y, 0.5f * w.x, 0.5f * w.y);
   }
-  for (int i = tid; i < S::RS; i += S::THREADS) {
-    const int s = i / 33, cc = i - 33 * s;
-    rs_tw[i] = cc < 32 ? root_q(twq, cc + 32 * s, N) : cpx{0.0f, 0.0f};
+  for (int i = tid; i < 16 * 33; i += S::THREADS) {
+    const int row = i / 33, cc = i - 33 * row, p = row >> 1, jj0 = row & 1;
+    if (cc < 32) {
+      const cpx u = root_q(twq, cc + 32 * (4 * p + jj0), N), w = root_q(twq, cc + 32 * (4 * p + 2 + jj0), N);
+      rs_tw[i] = make_float4(u.x, u.y, w.x, w.y);
+    } else {
+      rs_tw[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   }
   if (lanes) {
     for (int i = tid; i < nmel; i += S::THREADS) band_s[i] = __ldg(a.mel_band + i);
     for (int i = tid; i < TPF; i += S::THREADS) lane_s[i] = __ldg(a.mel_lane + i);
-    for (int i = tid; i < 33 * TPF; i += S::THREADS) lw_s[i] = __ldg(a.mel_lw + i);
+    for (int i = tid; i < 17 * TPF; i += S::THREADS) {
+      const int p = i / TPF, jj = i - p * TPF;
+      const float2 u = __ldg(a.mel_lw + 2 * p * TPF + jj);
+      const float2 w = 2 * p + 1 < 33 ? __ldg(a.mel_lw + (2 * p + 1) * TPF + jj) : make_float2(0.0f, 0.0f);
+      lw_s[i] = make_float4(u.x, u.y, w.x, w.y);
+    }
   } else if (mel_in_smem) {
     for (int i = tid; i < a.mel_nnz; i += S::THREADS) melw_s[i] = __ldg(a.mel_pw + i);
   }
@@ -783,12 +802,14 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
     }
     // ---- window
     {
-      const float2 *wb = reinterpret_cast<const float2 *>(win_s) + j;
+      const float4 *wb = win_s + j;
 #pragma unroll
-      for (int r = 0; r < 32; r++) {
-        const float2 w = wb[TPF * r];
+      for (int r = 0; r < 32; r += 2) {
+        const float4 w = wb[TPF * (r / 2)];
         v[r].x *= w.x;
         v[r].y *= w.y;
+        v[r + 1].x *= w.z;
+        v[r + 1].y *= w.w;
       }
     }
 
@@ -804,13 +825,18 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       dft16(e);
       dft16(o);
       cpx *row = fb + j * 33;
-      const cpx g16 = tw2[15 * TPF + j];  // W_M^(16 j)
+      const float4 t78 = tw4[7 * TPF + j];  // k = 15, 16
+      const cpx g16 = {t78.z, t78.w};      // W_M^(16 j)
+      float4 tp = t78;
       static_for<0, 16>([&](auto ki) {
         constexpr int k = decltype(ki)::value;
         const cpx tt = tw_const<k, 32>(o[k]);
         cpx lo = cadd(e[k], tt), hi = csub(e[k], tt);
         if constexpr (k > 0) {
-          const cpx tk = tw2[(k - 1) * TPF + j];
+          // pair k / 2 holds k (odd) and k + 1
+          if constexpr (k == 15) tp = t78;
+          else if constexpr (k % 2 == 1) tp = tw4[(k / 2) * TPF + j];
+          const cpx tk = (k % 2 == 1) ? cpx{tp.x, tp.y} : cpx{tp.z, tp.w};
           lo = cmul(lo, tk);
           hi = cmul(hi, cmul(tk, g16));
         } else {
@@ -852,6 +878,7 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
     {
       float *Pa = P + col + 33 * j0;                         // bin col + 32 s at col + 33 s
       float *Pb = P + (2111 - col - 33 * j0) + (c0 ? 1 : 0);  // bin M - col - 32 s
+      float4 rsp;
       static_for<0, 16>([&](auto ii) {
         constexpr int i = decltype(ii)::value;
         const cpx za = z[i];
@@ -860,7 +887,8 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
         else zb = c0 ? (j0 ? z[31 - i] : z[32 - i]) : rcv[15 - i];
         const float ex = za.x + zb.x, ey = za.y - zb.y;
         const float ox = za.y + zb.y, oy = zb.x - za.x;
-        const cpx w = rs_tw[66 * i + 33 * j0 + col];  // W_N^k
+        if constexpr (i % 2 == 0) rsp = rs_tw[(i + j0) * 33 + col];  // row 2 (i / 2) + j0
+        const cpx w = (i % 2 == 0) ? cpx{rsp.x, rsp.y} : cpx{rsp.z, rsp.w};  // W_N^k
         const float wr = fmaf(w.x, ox, -w.y * oy), wi = fmaf(w.x, oy, w.y * ox);
         const float xr = ex + wr, xi = ey + wi;
         const float yr = ex - wr, yi = ey - wi;
@@ -883,12 +911,14 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       const unsigned fl = (unsigned)li.x;
       int slot = li.y & 1023;
       const float *pl = P + 33 * j;
-      const float2 *wl = lw_s + j;
+      const float4 *wl = lw_s + j;
       float R = 0.0f, Fs = 0.0f, tot = 0.0f;
+      float4 wq;
 #pragma unroll
       for (int b = 0; b < 32; b++) {
         const float p = pl[b];
-        const float2 w = wl[b * TPF];
+        if ((b & 1) == 0) wq = wl[(b >> 1) * TPF];
+        const float2 w = (b & 1) ? make_float2(wq.z, wq.w) : make_float2(wq.x, wq.y);
         tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
@@ -900,7 +930,8 @@ __global__ void __launch_bounds__(W2Shape::THREADS, 1) frame_warp2_kernel(FrontA
       }
       if (j == TPF - 1) {
         const float p = pl[32];
-        const float2 w = wl[32 * TPF];
+        const float4 wn = wl[16 * TPF];
+        const float2 w = make_float2(wn.x, wn.y);
         tot = fmaf(p, 0.0f, tot);
         R = fmaf(w.x, p, R);
         Fs = fmaf(w.y, p, Fs);
@@ -1477,7 +1508,8 @@ cudaError_t launch_frontend_tc(const FrontArgs &a, int grid_limit, cudaStream_t 
 
 static cudaError_t launch_warp2(const FrontArgs &a, int grid_limit, cudaStream_t s, int *launched) {
   using S = W2Shape;
-  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * 34 * (size_t)S::TPF
+  // lane walk: band words, lane words (8 TPF), weight pairs (17 x TPF float4)
+  const size_t tables = a.mel_lane_ok ? align16(4 * (size_t)a.n_mels) + 8 * (size_t)S::TPF + 16 * 17 * (size_t)S::TPF
                                       : (a.mel_nnz <= S::MEL_SMEM_MAX ? align16(4 * (size_t)a.mel_nnz) : 0);
   const size_t smem = warp2_fixed_smem() + tables;
   int per_sm = 1, sms = 148;

@@ -540,3 +540,17 @@ def test_batch_mixing_short_and_long_clips_matches_single_calls():
         np.testing.assert_array_equal(o, M.mfcc(c, sr=SR, n_fft=2048, hop_length=512))
     exp = O.mfcc(clips[1], SR, 20, 2048, 512, 2048, 128)
     assert O.mfcc_rel_error(outs[1], exp) < MFCC_TOL
+
+
+@pytest.mark.parametrize("n_mels", [64, 80, 128])
+@pytest.mark.parametrize("n_mfcc", [1, 2, 5, 9, 13, 20, 24, 28, 32])
+def test_folded_dct_every_coefficient_group_vs_oracle(n_mels, n_mfcc):
+    """The folded cp.async DCT (64, 80 and 128 bands) for every number of
+    accumulators per coefficient group (KQ = ceil(ceil(n_mfcc / 2) / 2), 1..8)
+    and a clip whose last 64-frame tile is partial; n_mfcc above 32 falls to
+    the chunked kernels and is covered above."""
+    y = synth.music_clip(3 * SR + 1234, SR, seed=n_mels * 100 + n_mfcc)
+    got = M.mfcc(y, sr=SR, n_mfcc=n_mfcc, n_fft=2048, hop_length=512, n_mels=n_mels)
+    exp = O.mfcc(y, SR, n_mfcc, 2048, 512, 2048, n_mels)
+    assert got.shape == exp.shape
+    assert O.mfcc_rel_error(got, exp) < MFCC_TOL, O.mfcc_rel_error(got, exp)
